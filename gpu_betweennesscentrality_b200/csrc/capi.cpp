@@ -1,0 +1,300 @@
+// capi.cpp -- extern "C" boundary of libqbc_b200 (declared in include/qbc_b200.h).
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "../../include/qbc_b200.h"
+#include "device.h"
+#include "host.h"
+
+struct qbc_graph {
+  qbc::Graph g;
+};
+struct qbc_index {
+  qbc::Handle h;
+  ~qbc_index() { qbc::device_release(h); }
+};
+
+namespace {
+thread_local std::string g_err;
+
+template <class F>
+int guarded(F &&f) {
+  try {
+    f();
+    g_err.clear();
+    return QBC_OK;
+  } catch (const qbc::Error &e) {
+    g_err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    g_err = "host allocation failed";
+    return QBC_ENOMEM;
+  } catch (const std::exception &e) {
+    g_err = e.what();
+    return QBC_EINVAL;
+  }
+}
+
+void need(bool ok, const char *what) {
+  if (!ok) throw qbc::Error(QBC_EINVAL, what);
+}
+}  // namespace
+
+extern "C" {
+
+const char *qbc_last_error(void) { return g_err.c_str(); }
+const char *qbc_version(void) { return "qbc_b200 0.1 (sm_100a)"; }
+
+int qbc_graph_read(const char *path, qbc_graph **out) {
+  return guarded([&] {
+    need(path && out, "null argument");
+    auto p = std::make_unique<qbc_graph>();
+    p->g = qbc::graph_read(path);
+    *out = p.release();
+  });
+}
+
+int qbc_graph_from_lines(int n, int m, const int32_t *u1, const int32_t *v1, const int32_t *w, qbc_graph **out) {
+  return guarded([&] {
+    need(out && (m == 0 || (u1 && v1 && w)), "null argument");
+    auto p = std::make_unique<qbc_graph>();
+    p->g = qbc::graph_from_lines(n, m, u1, v1, w);
+    *out = p.release();
+  });
+}
+
+int qbc_graph_info(const qbc_graph *g, int32_t *n, int32_t *arcs) {
+  return guarded([&] {
+    need(g, "null graph");
+    if (n) *n = g->g.n;
+    if (arcs) *arcs = g->g.arcs();
+  });
+}
+
+int qbc_graph_arcs(const qbc_graph *g, int32_t *off, int32_t *head, int32_t *w) {
+  return guarded([&] {
+    need(g, "null graph");
+    if (off) std::memcpy(off, g->g.off.data(), g->g.off.size() * 4);
+    if (head) std::memcpy(head, g->g.head.data(), g->g.head.size() * 4);
+    if (w) std::memcpy(w, g->g.w.data(), g->g.w.size() * 4);
+  });
+}
+
+void qbc_graph_free(qbc_graph *g) { delete g; }
+
+int qbc_read_order(const char *path, int32_t n, int32_t *node_order) {
+  return guarded([&] {
+    need(path && node_order, "null argument");
+    auto o = qbc::read_order(path, n);
+    std::memcpy(node_order, o.data(), o.size() * 4);
+  });
+}
+
+int qbc_read_query(const char *path, int32_t n, int32_t cap, int32_t *q, int32_t *ids0) {
+  return guarded([&] {
+    need(path && q, "null argument");
+    auto ids = qbc::read_query(path, n);
+    *q = (int32_t)ids.size();
+    if (ids0) {
+      if ((int32_t)ids.size() > cap) throw qbc::Error(QBC_EINVAL, "query batch larger than the output capacity");
+      std::memcpy(ids0, ids.data(), ids.size() * 4);
+    }
+  });
+}
+
+int qbc_min_degree_order(const qbc_graph *g, int32_t *node_order) {
+  return guarded([&] {
+    need(g && node_order, "null argument");
+    auto o = qbc::min_degree_order(g->g);
+    std::memcpy(node_order, o.data(), o.size() * 4);
+  });
+}
+
+int qbc_index_build(const qbc_graph *g, int kind, const int32_t *node_order, int nthreads, qbc_index **out) {
+  return guarded([&] {
+    need(g && out, "null argument");
+    auto p = std::make_unique<qbc_index>();
+    if (kind == QBC_INDEX_MHL) {
+      p->h.host = qbc::build_mhl(g->g, nthreads);
+    } else if (kind == QBC_INDEX_H2H) {
+      need(node_order != nullptr, "H2H index needs a node order");
+      std::vector<int32_t> o(node_order, node_order + g->g.n);
+      p->h.host = qbc::build_h2h(g->g, o, nthreads);
+    } else {
+      throw qbc::Error(QBC_EINVAL, "unknown index kind");
+    }
+    *out = p.release();
+  });
+}
+
+int qbc_index_upload(qbc_index *idx, int device) {
+  return guarded([&] {
+    need(idx, "null index");
+    qbc::device_upload(idx->h, device);
+  });
+}
+
+int qbc_index_release_device(qbc_index *idx) {
+  return guarded([&] {
+    need(idx, "null index");
+    qbc::device_release(idx->h);
+  });
+}
+
+int qbc_index_info(const qbc_index *idx, int64_t *info) {
+  return guarded([&] {
+    need(idx && info, "null argument");
+    const qbc::Index &ix = idx->h.host;
+    info[0] = ix.n;
+    info[1] = (int64_t)ix.arc_head.size();
+    info[2] = ix.lab_off.empty() ? 0 : ix.lab_off[ix.n];
+    info[3] = ix.tree_height;
+    info[4] = ix.tree_width;
+    info[5] = qbc::device_bytes(idx->h);
+    info[6] = (int64_t)ix.kind;
+    info[7] = ix.depth_sum;
+  });
+}
+
+int qbc_index_scan_entries(const qbc_index *idx, const int32_t *sources0, int32_t ns, int64_t *entries) {
+  return guarded([&] {
+    need(idx && entries && (ns == 0 || sources0), "null argument");
+    for (int32_t i = 0; i < ns; i++)
+      if (sources0[i] < 0 || sources0[i] >= idx->h.host.n) throw qbc::Error(QBC_EINVAL, "source id out of range");
+    *entries = qbc::scan_entries(idx->h.host, sources0, ns);
+  });
+}
+
+void qbc_index_free(qbc_index *idx) { delete idx; }
+
+int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int32_t *send, int64_t *lab_off,
+                     int32_t *dis, int32_t *ch, int32_t *anc) {
+  return guarded([&] {
+    need(idx, "null index");
+    const qbc::Index &ix = idx->h.host;
+    auto cp = [](void *dst, const void *src, size_t bytes) {
+      if (dst && bytes) std::memcpy(dst, src, bytes);
+    };
+    cp(vid_of, ix.vid_of.data(), ix.vid_of.size() * 4);
+    cp(depth, ix.depth.data(), ix.depth.size() * 4);
+    cp(send, ix.send.data(), ix.send.size() * 4);
+    cp(lab_off, ix.lab_off.data(), ix.lab_off.size() * 8);
+    cp(dis, ix.dis.data(), ix.dis.size() * 4);
+    cp(ch, ix.ch.data(), ix.ch.size() * 4);
+    cp(anc, ix.anc.data(), ix.anc.size() * 4);
+  });
+}
+
+int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams) {
+  return guarded([&] {
+    need(idx && (nparams == 0 || params), "null argument");
+    qbc::Tuning &t = idx->h.tuning;
+    int32_t *f[] = {&t.lanes_per_source, &t.label_threads, &t.split, &t.chunk, &t.dep_threads};
+    if (nparams > 0) {
+      int32_t k = params[0];
+      need(k == 0 || k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32, "lanes per source must be 0 or a power of two <= 32");
+    }
+    const int32_t old_chunk = t.chunk;
+    for (int32_t i = 0; i < nparams && i < 5; i++) *f[i] = params[i];
+    if (nparams > 3 && t.chunk != old_chunk && idx->h.dev) qbc::device_upload(idx->h, qbc::device_id(idx->h));
+  });
+}
+
+int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams) {
+  return guarded([&] {
+    need(idx && (nparams == 0 || params), "null argument");
+    const qbc::Tuning &t = idx->h.tuning;
+    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads};
+    for (int32_t i = 0; i < nparams && i < 5; i++) params[i] = f[i];
+  });
+}
+
+int qbc_bc_all(qbc_index *idx, double *bc_out) {
+  return guarded([&] {
+    need(idx && bc_out, "null argument");
+    std::vector<int32_t> all((size_t)idx->h.host.n);
+    for (int32_t t = 0; t < idx->h.host.n; t++) all[t] = idx->h.host.vid_of[t];  // tid order
+    qbc::host_bc_sources(idx->h, all.data(), (int32_t)all.size(), bc_out);
+  });
+}
+
+int qbc_bc_sources(qbc_index *idx, const int32_t *sources0, int32_t ns, double *bc_out) {
+  return guarded([&] {
+    need(idx && bc_out && ns >= 0 && (ns == 0 || sources0), "null argument");
+    qbc::host_bc_sources(idx->h, sources0, ns, bc_out);
+  });
+}
+
+int qbc_bc_plain(qbc_index *idx, const int32_t *sources0, int32_t ns, double *bc_out) {
+  return guarded([&] {
+    need(idx && bc_out && ns >= 0 && (ns == 0 || sources0), "null argument");
+    qbc::host_bc_plain(idx->h, sources0, ns, bc_out);
+  });
+}
+
+int qbc_bc_sources_device(qbc_index *idx, const int32_t *d_sources0, int32_t ns, double *d_bc, void *stream) {
+  return guarded([&] {
+    need(idx && d_bc && ns >= 0 && (ns == 0 || d_sources0), "null argument");
+    qbc::device_bc_sources(idx->h, d_sources0, ns, d_bc, stream);
+  });
+}
+
+int qbc_bc_query(qbc_index *idx, const int32_t *points0, int32_t q, double *out) {
+  return guarded([&] {
+    need(idx && q >= 0 && (q == 0 || (points0 && out)), "null argument");
+    const int32_t n = idx->h.host.n;
+    for (int32_t i = 0; i < q; i++)
+      if (points0[i] < 0 || points0[i] >= n) throw qbc::Error(QBC_EINVAL, "query id out of range");
+    std::vector<double> bc((size_t)n);
+    std::vector<int32_t> all((size_t)n);
+    for (int32_t t = 0; t < n; t++) all[t] = idx->h.host.vid_of[t];
+    qbc::host_bc_sources(idx->h, all.data(), n, bc.data());
+    for (int32_t i = 0; i < q; i++) out[i] = bc[points0[i]];
+  });
+}
+
+int qbc_bc_query_batch(qbc_index *idx, const int32_t *points0, const int32_t *set_off, int32_t nsets,
+                       const int32_t *sources0, int32_t ns, double *out) {
+  return guarded([&] {
+    need(idx && set_off && nsets >= 0, "null argument");
+    const int32_t n = idx->h.host.n;
+    const int32_t total = nsets ? set_off[nsets] : 0;
+    need(total == 0 || (points0 && out), "null argument");
+    for (int32_t i = 0; i < total; i++)
+      if (points0[i] < 0 || points0[i] >= n) throw qbc::Error(QBC_EINVAL, "query id out of range");
+    std::vector<double> bc((size_t)n);
+    if (sources0) {
+      qbc::host_bc_sources(idx->h, sources0, ns, bc.data());
+    } else {
+      std::vector<int32_t> all((size_t)n);
+      for (int32_t t = 0; t < n; t++) all[t] = idx->h.host.vid_of[t];
+      qbc::host_bc_sources(idx->h, all.data(), n, bc.data());
+    }
+    for (int32_t i = 0; i < total; i++) out[i] = bc[points0[i]];
+  });
+}
+
+int qbc_index_profile(qbc_index *idx, int on) {
+  return guarded([&] {
+    need(idx, "null index");
+    qbc::device_profiling(idx->h, on != 0);
+  });
+}
+
+int qbc_index_stats(qbc_index *idx, double *out) {
+  return guarded([&] {
+    need(idx && out, "null argument");
+    qbc::device_stats(idx->h, out);
+  });
+}
+
+int qbc_rows(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *dist, uint32_t *cnt, int32_t *hop) {
+  return guarded([&] {
+    need(idx && dist && ns >= 0 && (ns == 0 || sources0), "null argument");
+    qbc::host_rows(idx->h, sources0, ns, dist, cnt, hop);
+  });
+}
+
+}  // extern "C"

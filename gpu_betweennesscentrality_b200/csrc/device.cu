@@ -1,0 +1,956 @@
+// device.cu -- B200 (sm_100a) kernels and drivers of libqbc_b200.
+//
+// Per source s the reference runs, inside one CTA (MHLQBC.cu:237-475): LCA of s with every tree
+// node, a dist/count/hop label scan per target, SP-DAG arcs with layer counts, a layer queue and a
+// layered FP64 backprop.  Here the same quantities come from three kernels:
+//
+//   k_label_scan   (K1+K2)  G sources x a range of targets per CTA.  The G source rows (label
+//                  distances, ancestor ids and subtree ends) sit in shared memory; each target row
+//                  is read once from HBM/L2 per G sources (16-byte vector loads) and reused by all
+//                  of them.  LCA depth = binary search of the target id in the source's nested
+//                  ancestor intervals (DFS preorder), replacing the Euler-tour RMQ gathers.  The
+//                  scan tracks min + tie flag; path counts and hops are gathered only at the
+//                  minimising entries, so the hot loop reads 4 B per entry instead of 12.
+//   k_dependency   (K3-K5)  one CTA per source: layer histogram with warp-aggregated shared
+//                  atomics, block scan, scatter into a level queue, then a pull-form backprop
+//                  (each vertex sums over its own DAG out-arcs, no FP64 atomics on delta) and
+//                  an FP64 red into BC.
+//   k_kahn_dependency (QBC) distance-only rows from the H2H index; sigma and topological waves
+//                  by a device Kahn pass (QBC.cu:485-555 ran it on the host), then the same backprop.
+//
+// Chunks of sources are double-buffered over two streams so the compute-bound label scan of chunk
+// k+1 overlaps the latency-bound dependency pass of chunk k.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/qbc_b200.h"
+#include "device.h"
+
+namespace qbc {
+
+#define CK(call)                                                                                    \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess)                                                                          \
+      throw Error(e_ == cudaErrorMemoryAllocation ? QBC_ENOMEM : QBC_ECUDA,                         \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                              \
+  } while (0)
+
+enum : int32_t { ERR_NONE = 0, ERR_HOP_CAP = 1, ERR_DISCONNECTED = 2, ERR_BAD_SOURCE = 3 };
+
+constexpr int kLayerCap = 4094;  // shared-memory layer counters; deeper DAGs use global memory
+constexpr unsigned kFull = 0xffffffffu;
+
+// ------------------------------------------------------------------------------- state
+struct DeviceState {
+  int device = 0;
+  cudaStream_t s_label = nullptr, s_dep = nullptr;
+  cudaEvent_t ev_label[2] = {nullptr, nullptr}, ev_dep[2] = {nullptr, nullptr}, ev_start = nullptr;
+  int32_t n = 0, n_pad = 0, hmax_pad = 0;
+  int32_t *depth = nullptr, *send = nullptr, *arc_off = nullptr, *arc_head = nullptr, *arc_w = nullptr;
+  int32_t *vid_of = nullptr, *tid_of = nullptr, *dis = nullptr, *anc = nullptr;
+  int64_t *lab_off = nullptr;
+  int2 *ch = nullptr;
+  // scratch, two buffers of `chunk` slots
+  int32_t chunk = 0;
+  int2 *dc[2] = {nullptr, nullptr};
+  int32_t *hop[2] = {nullptr, nullptr};
+  double *delta[2] = {nullptr, nullptr};
+  int32_t *order[2] = {nullptr, nullptr};
+  int32_t *lcnt[2] = {nullptr, nullptr};
+  int32_t *src[2] = {nullptr, nullptr};
+  double *bc_tid = nullptr;
+  double *bc_vid = nullptr;
+  int32_t *sources = nullptr;  // staging for host source lists
+  int32_t sources_cap = 0;
+  int32_t *err = nullptr;
+  int64_t bytes = 0;
+  int smem_optin = 0;
+  // optional per-launch timing of the two main kernels (events on their launching streams)
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_lab, ev_dp;
+  size_t ev_lab_used = 0, ev_dp_used = 0;
+  double label_ms = 0.0, dep_ms = 0.0;
+  int64_t label_launches = 0, dep_launches = 0, launches = 0;
+};
+
+static std::pair<cudaEvent_t, cudaEvent_t> take_events(std::vector<std::pair<cudaEvent_t, cudaEvent_t>> &pool,
+                                                       size_t &used) {
+  if (used == pool.size()) {
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    pool.push_back({a, b});
+  }
+  return pool[used++];
+}
+
+template <class T>
+static T *dmalloc(DeviceState *d, size_t count) {
+  void *p = nullptr;
+  if (count == 0) count = 1;
+  CK(cudaMalloc(&p, count * sizeof(T)));
+  d->bytes += (int64_t)(count * sizeof(T));
+  return (T *)p;
+}
+
+template <class T>
+static T *dupload(DeviceState *d, const std::vector<T> &v, cudaStream_t s) {
+  T *p = dmalloc<T>(d, v.size());
+  if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  return p;
+}
+
+// ------------------------------------------------------------------------------- K1 + K2
+struct LabelArgs {
+  const int32_t *__restrict__ dis;
+  const int2 *__restrict__ ch;
+  const int32_t *__restrict__ anc;
+  const int64_t *__restrict__ lab_off;
+  const int32_t *__restrict__ depth;
+  const int32_t *__restrict__ send;
+  const int32_t *__restrict__ src;  // tids of this chunk's sources
+  int32_t ns, n, n_pad, stride, split;
+  int2 *__restrict__ out_dc;      // [ns][n_pad] (dist, count bits)
+  int32_t *__restrict__ out_hop;  // [ns][n_pad]
+};
+
+// largest J with lo[J] <= t < hi[J] (entry 0 is the root and always holds), returned as J+1
+__device__ __forceinline__ int lca_depth(const int32_t *lo, const int32_t *hi, int hs, int t) {
+  int l = 0, h = hs;
+  while (h - l > 1) {
+    int mid = (l + h) >> 1;
+    bool p = (lo[mid] <= t) && (t < hi[mid]);
+    l = p ? mid : l;
+    h = p ? h : mid;
+  }
+  return l + 1;
+}
+
+template <int K, bool COUNTS>
+__global__ void __launch_bounds__(256, 1) k_label_scan(LabelArgs a) {
+  constexpr int G = 32 / K;
+  extern __shared__ int4 smem4[];
+  int32_t *sm = reinterpret_cast<int32_t *>(smem4);
+  const int S = a.stride;
+  int32_t *s_dis = sm;
+  int32_t *s_lo = s_dis + G * S;
+  int32_t *s_hi = s_lo + G * S;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  int32_t *tbuf = s_hi + G * S + warp * S;
+  __shared__ int32_t s_tid[G], s_h[G];
+  __shared__ int64_t s_off[G];
+
+  const int first = blockIdx.y * G;
+  if (first >= a.ns) return;
+  const int gcount = min(G, a.ns - first);
+  if (threadIdx.x < G) {
+    int i = threadIdx.x;
+    int s = i < gcount ? a.src[first + i] : 0;
+    s_tid[i] = s;
+    s_h[i] = i < gcount ? a.depth[s] : 0;
+    s_off[i] = a.lab_off[s];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < G * S; idx += blockDim.x) {
+    const int i = idx / S, j = idx - i * S;
+    int vd = 0x3fffffff, vlo = INT_MAX, vhi = -1;
+    if (i < gcount && j < s_h[i]) {
+      vd = a.dis[s_off[i] + j];
+      vlo = a.anc[s_off[i] + j];
+      vhi = a.send[vlo];
+    }
+    s_dis[idx] = vd;
+    s_lo[idx] = vlo;
+    s_hi[idx] = vhi;
+  }
+  __syncthreads();
+
+  const int si = lane / K, kq = lane % K;
+  const bool have = si < gcount;
+  const int hs = have ? s_h[si] : 1;
+  const int64_t soff = s_off[si];
+  const int32_t *srow = s_dis + si * S;
+  const int32_t *slo = s_lo + si * S;
+  const int32_t *shi = s_hi + si * S;
+
+  const int nchunk = a.n_pad >> 3;
+  const int cbeg = (int)((int64_t)nchunk * blockIdx.x / a.split);
+  const int cend = (int)((int64_t)nchunk * (blockIdx.x + 1) / a.split);
+  for (int c = cbeg + warp; c < cend; c += nwarps) {
+    const int t0 = c << 3;
+    int rd[8], rc[8], rh[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int t = t0 + k;
+      rd[k] = 0; rc[k] = 0; rh[k] = 0;
+      if (t < a.n) {
+        const int64_t toff = a.lab_off[t];
+        const int hl = have ? lca_depth(slo, shi, hs, t) : 0;
+        const int H = __reduce_max_sync(kFull, hl);
+        for (int j = lane * 4; j < H; j += 128)
+          *reinterpret_cast<int4 *>(tbuf + j) = __ldg(reinterpret_cast<const int4 *>(a.dis + toff + j));
+        __syncwarp();
+        if (K == 1) {
+          int m = INT_MAX, jm = 0;
+          bool tie = false;
+          for (int j = 0; j < hl; j += 4) {
+            const int4 x = *reinterpret_cast<const int4 *>(srow + j);
+            const int4 y = *reinterpret_cast<const int4 *>(tbuf + j);
+            int v0 = x.x + y.x, v1 = x.y + y.y, v2 = x.z + y.z, v3 = x.w + y.w;
+            v1 = (j + 1 < hl) ? v1 : INT_MAX;
+            v2 = (j + 2 < hl) ? v2 : INT_MAX;
+            v3 = (j + 3 < hl) ? v3 : INT_MAX;
+#define QBC_STEP(v, jj)              \
+  if (v < m) {                       \
+    m = v; jm = jj; tie = false;     \
+  } else if (v == m) {               \
+    tie = true;                      \
+  }
+            QBC_STEP(v0, j) QBC_STEP(v1, j + 1) QBC_STEP(v2, j + 2) QBC_STEP(v3, j + 3)
+#undef QBC_STEP
+          }
+          rd[k] = m;
+          if (COUNTS && have) {
+            if (!tie) {
+              const int2 cs = __ldg(a.ch + soff + jm), ct = __ldg(a.ch + toff + jm);
+              rc[k] = (int)((unsigned)cs.x * (unsigned)ct.x);
+              rh[k] = cs.y + ct.y;
+            } else {
+              unsigned cc = 0;
+              int hh = 0;
+              for (int j = 0; j < hl; j++) {
+                if (srow[j] + tbuf[j] == m) {
+                  const int2 cs = __ldg(a.ch + soff + j), ct = __ldg(a.ch + toff + j);
+                  cc += (unsigned)cs.x * (unsigned)ct.x;
+                  hh = max(hh, cs.y + ct.y);
+                }
+              }
+              rc[k] = (int)cc;
+              rh[k] = hh;
+            }
+          }
+        } else {
+          int m = INT_MAX;
+          for (int j = kq * 4; j < hl; j += 4 * K) {
+            const int4 x = *reinterpret_cast<const int4 *>(srow + j);
+            const int4 y = *reinterpret_cast<const int4 *>(tbuf + j);
+            int v0 = x.x + y.x, v1 = x.y + y.y, v2 = x.z + y.z, v3 = x.w + y.w;
+            v1 = (j + 1 < hl) ? v1 : INT_MAX;
+            v2 = (j + 2 < hl) ? v2 : INT_MAX;
+            v3 = (j + 3 < hl) ? v3 : INT_MAX;
+            m = min(m, min(min(v0, v1), min(v2, v3)));
+          }
+#pragma unroll
+          for (int o = K / 2; o >= 1; o >>= 1) m = min(m, __shfl_xor_sync(kFull, m, o));
+          rd[k] = m;
+          if (COUNTS) {
+            unsigned cc = 0;
+            int hh = 0;
+            for (int j = kq * 4; j < hl; j += 4 * K) {
+#pragma unroll
+              for (int q = 0; q < 4; q++) {
+                if (j + q < hl && srow[j + q] + tbuf[j + q] == m) {
+                  const int2 cs = __ldg(a.ch + soff + j + q), ct = __ldg(a.ch + toff + j + q);
+                  cc += (unsigned)cs.x * (unsigned)ct.x;
+                  hh = max(hh, cs.y + ct.y);
+                }
+              }
+            }
+#pragma unroll
+            for (int o = K / 2; o >= 1; o >>= 1) {
+              cc += __shfl_xor_sync(kFull, cc, o);
+              hh = max(hh, __shfl_xor_sync(kFull, hh, o));
+            }
+            rc[k] = (int)cc;
+            rh[k] = hh;
+          }
+        }
+        __syncwarp();
+      }
+    }
+    if (have && kq == 0) {
+      const size_t slot = (size_t)(first + si);
+      int4 *od = reinterpret_cast<int4 *>(a.out_dc + slot * a.n_pad + t0);
+      od[0] = make_int4(rd[0], rc[0], rd[1], rc[1]);
+      od[1] = make_int4(rd[2], rc[2], rd[3], rc[3]);
+      od[2] = make_int4(rd[4], rc[4], rd[5], rc[5]);
+      od[3] = make_int4(rd[6], rc[6], rd[7], rc[7]);
+      if (COUNTS) {
+        int4 *oh = reinterpret_cast<int4 *>(a.out_hop + slot * a.n_pad + t0);
+        oh[0] = make_int4(rh[0], rh[1], rh[2], rh[3]);
+        oh[1] = make_int4(rh[4], rh[5], rh[6], rh[7]);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------- K3 - K5
+struct DepArgs {
+  const int32_t *__restrict__ arc_off;
+  const int32_t *__restrict__ arc_head;
+  const int32_t *__restrict__ arc_w;
+  const int32_t *__restrict__ src;
+  int32_t ns, n, n_pad;
+  int2 *dc;        // [ns][n_pad] (dist, sigma); sigma written by the Kahn kernel
+  int32_t *hop;    // [ns][n_pad] layer (MHL) / indegree then wave (H2H)
+  double *delta;   // [ns][n_pad]
+  int32_t *order;  // [ns][n_pad] level queue
+  int32_t *lcnt;   // [ns][2*(n_pad+2)] global layer counters when shared ones do not suffice
+  double *bc;      // [n] tid order, FP64 red target
+  int32_t *err;
+};
+
+__device__ __forceinline__ int block_reduce_max(int v, int *red) {
+  v = __reduce_max_sync(kFull, v);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int x = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : INT_MIN;
+    x = __reduce_max_sync(kFull, x);
+    if (threadIdx.x == 0) red[32] = x;
+  }
+  __syncthreads();
+  int r = red[32];
+  __syncthreads();
+  return r;
+}
+
+// exclusive scan of cnt[0..len) into itself; cnt[len] = total.  Block-wide.
+__device__ void block_exclusive_scan(int *cnt, int len, int *red) {
+  const int nt = blockDim.x;
+  const int per = (len + nt - 1) / nt;
+  const int b = threadIdx.x * per, e = min(len, b + per);
+  int local = 0;
+  for (int i = b; i < e; i++) local += cnt[i];
+  // block scan of `local`
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int x = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) red[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int nw = nt >> 5;
+    int w = lane < nw ? red[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(kFull, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) red[lane] = w;  // inclusive warp totals
+  }
+  __syncthreads();
+  int run = x - local + (warp > 0 ? red[warp - 1] : 0);
+  for (int i = b; i < e; i++) {
+    int c = cnt[i];
+    cnt[i] = run;
+    run += c;
+  }
+  __syncthreads();
+  if (threadIdx.x == nt - 1) cnt[len] = run;
+  __syncthreads();
+}
+
+// warp-aggregated atomicAdd of 1 on ctr[key]; returns this lane's slot.  `act` = lanes calling.
+__device__ __forceinline__ int agg_inc(int *ctr, int key, unsigned act) {
+  const unsigned grp = __match_any_sync(act, key);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(grp) - 1;
+  const int rank = __popc(grp & ((1u << lane) - 1u));
+  int base = 0;
+  if (lane == leader) base = atomicAdd(ctr + key, __popc(grp));
+  base = __shfl_sync(grp, base, leader);
+  return base + rank;
+}
+
+// Pull-form dependency of vertex v (MHLQBC.cu:452-466): delta(v) = sum over DAG arcs v->w of
+// sigma_v * (1 + delta_w) / sigma_w, operation order as the reference (:457).
+__device__ __forceinline__ double pull_delta(const DepArgs &a, const int2 *dc, const double *delta, int v) {
+  const int2 dv = dc[v];
+  const double sv = (double)dv.y;
+  double acc = 0.0;
+  const int e1 = a.arc_off[v + 1];
+  for (int e = a.arc_off[v]; e < e1; e++) {
+    const int w = a.arc_head[e];
+    const int2 dw = dc[w];
+    if (dw.x == dv.x + a.arc_w[e]) acc += sv * (1.0 + delta[w]) / (double)dw.y;
+  }
+  return acc;
+}
+
+__device__ void backprop_levels(const DepArgs &a, const int2 *dc, double *delta, const int32_t *order,
+                                const int *start, int maxL) {
+  for (int L = maxL; L >= 1; --L) {
+    const int b = start[L], e = start[L + 1];
+    for (int idx = b + threadIdx.x; idx < e; idx += blockDim.x) {
+      const int v = order[idx];
+      const double d = pull_delta(a, dc, delta, v);
+      delta[v] = d;
+      atomicAdd(a.bc + v, 0.5 * d);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_dependency(DepArgs a) {
+  __shared__ int sh_cnt[kLayerCap + 2];
+  __shared__ int sh_cur[kLayerCap + 2];
+  __shared__ int red[33];
+  const int slot = blockIdx.x;
+  if (slot >= a.ns) return;
+  const int s = a.src[slot];
+  const size_t base = (size_t)slot * a.n_pad;
+  const int2 *dc = a.dc + base;
+  const int32_t *hop = a.hop + base;
+  double *delta = a.delta + base;
+  int32_t *order = a.order + base;
+
+  int mx = 0;
+  for (int v = threadIdx.x; v < a.n; v += blockDim.x) mx = max(mx, hop[v]);
+  const int maxL = block_reduce_max(mx, red);
+  int *cnt = sh_cnt, *cur = sh_cur;
+  if (maxL + 2 > kLayerCap) {
+    cnt = a.lcnt + (size_t)slot * 2 * (a.n_pad + 2);
+    cur = cnt + (a.n_pad + 2);
+  }
+  for (int i = threadIdx.x; i <= maxL + 1; i += blockDim.x) cnt[i] = 0;
+  __syncthreads();
+  const int nround = (a.n + blockDim.x - 1) / blockDim.x * blockDim.x;
+  for (int v0 = 0; v0 < nround; v0 += blockDim.x) {
+    const int v = v0 + threadIdx.x;
+    const bool ok = v < a.n && v != s;
+    const unsigned act = __ballot_sync(kFull, ok);
+    if (ok) agg_inc(cnt, hop[v], act);
+  }
+  __syncthreads();
+  block_exclusive_scan(cnt, maxL + 1, red);
+  for (int i = threadIdx.x; i <= maxL + 1; i += blockDim.x) cur[i] = cnt[i];
+  __syncthreads();
+  for (int v0 = 0; v0 < nround; v0 += blockDim.x) {
+    const int v = v0 + threadIdx.x;
+    const bool ok = v < a.n && v != s;
+    const unsigned act = __ballot_sync(kFull, ok);
+    if (ok) {
+      const int pos = agg_inc(cur, hop[v], act);
+      order[pos] = v;
+    }
+  }
+  __syncthreads();
+  backprop_levels(a, dc, delta, order, cnt, maxL);
+}
+
+// QBC: sigma by Kahn waves on the SP-DAG from H2H distances (QBC.cu:335-344, :485-555), then
+// the same backprop.  hop[] holds the in-degree until a vertex is queued, then its wave.
+__global__ void __launch_bounds__(256) k_kahn_dependency(DepArgs a) {
+  __shared__ int sh_wave[kLayerCap + 2];
+  __shared__ int s_tail, s_flag;
+  const int slot = blockIdx.x;
+  if (slot >= a.ns) return;
+  const int s = a.src[slot];
+  const size_t base = (size_t)slot * a.n_pad;
+  int2 *dc = a.dc + base;
+  int32_t *deg = a.hop + base;
+  double *delta = a.delta + base;
+  int32_t *order = a.order + base;
+  int *wave = sh_wave;
+  bool global_waves = false;
+  int wave_cap = kLayerCap;
+  // in-degree over reverse arcs (arcs are symmetric) and sigma = 0
+  for (int v = threadIdx.x; v < a.n; v += blockDim.x) {
+    const int dv = dc[v].x;
+    int c = 0;
+    for (int e = a.arc_off[v]; e < a.arc_off[v + 1]; e++) {
+      const int u = a.arc_head[e];
+      if (dc[u].x + a.arc_w[e] == dv) c++;
+    }
+    deg[v] = c;
+    dc[v].y = (v == s) ? 1 : 0;
+  }
+  if (threadIdx.x == 0) {
+    order[0] = s;
+    deg[s] = 0;
+    s_tail = 1;
+    s_flag = 0;
+    wave[0] = 0;
+    wave[1] = 1;
+  }
+  __syncthreads();
+  int L = 0;
+  for (;;) {
+    const int b = wave[L], e = wave[L + 1];
+    if (b == e) break;
+    for (int idx = b + threadIdx.x; idx < e; idx += blockDim.x) {
+      const int v = order[idx];
+      const int2 dv = dc[v];
+      for (int ee = a.arc_off[v]; ee < a.arc_off[v + 1]; ee++) {
+        const int w = a.arc_head[ee];
+        if (dc[w].x == dv.x + a.arc_w[ee]) {
+          atomicAdd(&dc[w].y, dv.y);
+          if (atomicSub(&deg[w], 1) == 1) {
+            const int pos = atomicAdd(&s_tail, 1);
+            order[pos] = w;
+            deg[w] = L + 1;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (!global_waves && L + 2 >= wave_cap) {
+        // move wave starts to global memory
+        int *g = a.lcnt + (size_t)slot * 2 * (a.n_pad + 2);
+        for (int i = 0; i <= L + 1; i++) g[i] = wave[i];
+        s_flag = 1;
+      }
+    }
+    __syncthreads();
+    if (s_flag && !global_waves) {
+      wave = a.lcnt + (size_t)slot * 2 * (a.n_pad + 2);
+      global_waves = true;
+      wave_cap = a.n_pad + 2;
+    }
+    if (threadIdx.x == 0) wave[L + 2] = s_tail;
+    __syncthreads();
+    L++;
+    if (L > a.n) break;
+  }
+  if (threadIdx.x == 0) deg[s] = 0;
+  if (s_tail != a.n) {
+    if (threadIdx.x == 0) atomicCAS(a.err, ERR_NONE, ERR_DISCONNECTED);
+    return;
+  }
+  __syncthreads();
+  // waves 1..L-1 hold vertices; wave L is empty
+  backprop_levels(a, dc, delta, order, wave, L - 1);
+}
+
+__global__ void k_tid_to_vid_f64(const double *__restrict__ in, const int32_t *__restrict__ vid_of, double *out,
+                                 int n, int accumulate) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int v = vid_of[t];
+    out[v] = accumulate ? out[v] + in[t] : in[t];
+  }
+}
+
+__global__ void k_vid_to_tid(const int32_t *__restrict__ vids, const int32_t *__restrict__ tid_of, int32_t *out,
+                             int ns, int n, int32_t *err) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {
+    const int v = vids[i];
+    const bool ok = v >= 0 && v < n;
+    out[i] = ok ? tid_of[v] : 0;
+    if (!ok) atomicCAS(err, ERR_NONE, ERR_BAD_SOURCE);
+  }
+}
+
+__global__ void k_rows_to_vid(const int2 *__restrict__ dc, const int32_t *__restrict__ hop,
+                              const int32_t *__restrict__ vid_of, int n, int n_pad, int ns, int32_t *dist,
+                              uint32_t *cnt, int32_t *hp) {
+  const int slot = blockIdx.y;
+  if (slot >= ns) return;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int v = vid_of[t];
+    const int2 x = dc[(size_t)slot * n_pad + t];
+    dist[(size_t)slot * n + v] = x.x;
+    if (cnt) cnt[(size_t)slot * n + v] = (uint32_t)x.y;
+    if (hp) hp[(size_t)slot * n + v] = hop[(size_t)slot * n_pad + t];
+  }
+}
+
+// ------------------------------------------------------------------------------- launch config
+struct LabelPlan {
+  int K, G, S, threads, split;
+  size_t smem;
+};
+
+static LabelPlan plan_label(const Handle &h, const DeviceState *d, int32_t ns, bool plain) {
+  LabelPlan p{};
+  p.threads = std::max(64, std::min(256, (h.tuning.label_threads / 32) * 32));
+  p.S = d->hmax_pad;
+  const size_t budget = (size_t)std::max(48 * 1024, d->smem_optin) - 2048;
+  const size_t tb = (size_t)(p.threads / 32) * p.S * 4;
+  int K = h.tuning.lanes_per_source;
+  if (plain) K = 32;
+  if (K <= 0) {
+    K = 1;
+    while (K < 32 && ((size_t)(32 / K) * 3 * p.S * 4 + tb > budget)) K *= 2;
+  }
+  p.K = K;
+  p.G = 32 / K;
+  p.smem = (size_t)p.G * 3 * p.S * 4 + tb;
+  if (p.smem > budget) throw Error(QBC_EDEVICE, "tree height " + std::to_string(h.host.tree_height) + " exceeds the label kernel's shared-memory capacity");
+  const int groups = (ns + p.G - 1) / p.G;
+  int split = h.tuning.split;
+  if (split <= 0) {
+    // ~8 CTAs per SM in flight over the chunk, at least 1 target chunk of 8 per warp
+    const int want = 148 * 8;
+    split = std::max(1, (want + groups - 1) / groups);
+    split = std::min(split, std::max(1, (d->n_pad / 8) / (p.threads / 32)));
+  }
+  p.split = split;
+  return p;
+}
+
+template <int K, bool C>
+static void launch_label_k(const LabelPlan &p, const LabelArgs &a, int groups, cudaStream_t st) {
+  auto kern = k_label_scan<K, C>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem));
+  dim3 grid(p.split, groups);
+  kern<<<grid, p.threads, p.smem, st>>>(a);
+  CK(cudaGetLastError());
+}
+
+template <bool C>
+static void launch_label_c(const LabelPlan &p, const LabelArgs &a, int groups, cudaStream_t st) {
+  switch (p.K) {
+    case 1: launch_label_k<1, C>(p, a, groups, st); break;
+    case 2: launch_label_k<2, C>(p, a, groups, st); break;
+    case 4: launch_label_k<4, C>(p, a, groups, st); break;
+    case 8: launch_label_k<8, C>(p, a, groups, st); break;
+    case 16: launch_label_k<16, C>(p, a, groups, st); break;
+    default: launch_label_k<32, C>(p, a, groups, st); break;
+  }
+}
+
+static void launch_label(const Handle &h, DeviceState *d, int buf, int32_t ns, bool plain, cudaStream_t st) {
+  LabelPlan p = plan_label(h, d, ns, plain);
+  LabelArgs a{};
+  a.dis = d->dis;
+  a.ch = d->ch;
+  a.anc = d->anc;
+  a.lab_off = d->lab_off;
+  a.depth = d->depth;
+  a.send = d->send;
+  a.src = d->src[buf];
+  a.ns = ns;
+  a.n = d->n;
+  a.n_pad = d->n_pad;
+  a.stride = p.S;
+  a.split = p.split;
+  a.out_dc = d->dc[buf];
+  a.out_hop = d->hop[buf];
+  const int groups = (ns + p.G - 1) / p.G;
+  std::pair<cudaEvent_t, cudaEvent_t> ev{};
+  if (d->profiling) {
+    ev = take_events(d->ev_lab, d->ev_lab_used);
+    CK(cudaEventRecord(ev.first, st));
+  }
+  if (h.host.kind == IndexKind::MHL) launch_label_c<true>(p, a, groups, st);
+  else launch_label_c<false>(p, a, groups, st);
+  if (d->profiling) CK(cudaEventRecord(ev.second, st));
+  d->label_launches++;
+  d->launches++;
+}
+
+static DepArgs dep_args(DeviceState *d, int buf, int32_t ns) {
+  DepArgs a{};
+  a.arc_off = d->arc_off;
+  a.arc_head = d->arc_head;
+  a.arc_w = d->arc_w;
+  a.src = d->src[buf];
+  a.ns = ns;
+  a.n = d->n;
+  a.n_pad = d->n_pad;
+  a.dc = d->dc[buf];
+  a.hop = d->hop[buf];
+  a.delta = d->delta[buf];
+  a.order = d->order[buf];
+  a.lcnt = d->lcnt[buf];
+  a.bc = d->bc_tid;
+  a.err = d->err;
+  return a;
+}
+
+static void launch_dep(const Handle &h, DeviceState *d, int buf, int32_t ns, cudaStream_t st) {
+  DepArgs a = dep_args(d, buf, ns);
+  const int threads = std::max(64, std::min(256, (h.tuning.dep_threads / 32) * 32));
+  std::pair<cudaEvent_t, cudaEvent_t> ev{};
+  if (d->profiling) {
+    ev = take_events(d->ev_dp, d->ev_dp_used);
+    CK(cudaEventRecord(ev.first, st));
+  }
+  if (h.host.kind == IndexKind::MHL) k_dependency<<<ns, threads, 0, st>>>(a);
+  else k_kahn_dependency<<<ns, threads, 0, st>>>(a);
+  CK(cudaGetLastError());
+  if (d->profiling) CK(cudaEventRecord(ev.second, st));
+  d->dep_launches++;
+  d->launches++;
+}
+
+// ------------------------------------------------------------------------------- upload
+void device_upload(Handle &h, int device) {
+  device_release(h);
+  const Index &ix = h.host;
+  CK(cudaSetDevice(device));
+  DeviceState *d = new DeviceState();
+  h.dev = d;
+  d->device = device;
+  try {
+    CK(cudaStreamCreateWithFlags(&d->s_label, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&d->s_dep, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; b++) {
+      CK(cudaEventCreateWithFlags(&d->ev_label[b], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&d->ev_dep[b], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&d->ev_start, cudaEventDisableTiming));
+    CK(cudaDeviceGetAttribute(&d->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    d->n = ix.n;
+    d->n_pad = (ix.n + 7) & ~7;
+    int S = (ix.tree_height + 3) & ~3;
+    if (((S / 4) & 1) == 0) S += 4;  // odd number of 16-byte groups: conflict-free LDS.128 across rows
+    d->hmax_pad = S;
+    cudaStream_t st = d->s_label;
+    d->depth = dupload(d, ix.depth, st);
+    d->send = dupload(d, ix.send, st);
+    d->arc_off = dupload(d, ix.arc_off, st);
+    d->arc_head = dupload(d, ix.arc_head, st);
+    d->arc_w = dupload(d, ix.arc_w, st);
+    d->vid_of = dupload(d, ix.vid_of, st);
+    d->tid_of = dupload(d, ix.tid_of, st);
+    d->lab_off = dupload(d, ix.lab_off, st);
+    d->dis = dupload(d, ix.dis, st);
+    d->anc = dupload(d, ix.anc, st);
+    if (ix.kind == IndexKind::MHL) {
+      d->ch = dmalloc<int2>(d, ix.ch.size() / 2);
+      CK(cudaMemcpyAsync(d->ch, ix.ch.data(), ix.ch.size() * 4, cudaMemcpyHostToDevice, st));
+    }
+    // scratch: two buffers of `chunk` source slots
+    const size_t per_slot = (size_t)d->n_pad * (8 + 4 + 8 + 4) + (size_t)2 * (d->n_pad + 2) * 4 + 4;
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    int32_t chunk = h.tuning.chunk;
+    if (chunk <= 0) {
+      const size_t budget = std::min<size_t>(free_b / 4, (size_t)24 << 30);
+      chunk = (int32_t)std::max<size_t>(32, std::min<size_t>(4096, budget / (2 * per_slot)));
+      chunk = std::max(32, (chunk / 32) * 32);
+    }
+    chunk = std::min<int32_t>(chunk, std::max(32, (ix.n + 31) / 32 * 32));
+    d->chunk = chunk;
+    for (int b = 0; b < 2; b++) {
+      d->dc[b] = dmalloc<int2>(d, (size_t)chunk * d->n_pad);
+      d->hop[b] = dmalloc<int32_t>(d, (size_t)chunk * d->n_pad);
+      d->delta[b] = dmalloc<double>(d, (size_t)chunk * d->n_pad);
+      d->order[b] = dmalloc<int32_t>(d, (size_t)chunk * d->n_pad);
+      d->lcnt[b] = dmalloc<int32_t>(d, (size_t)chunk * 2 * (d->n_pad + 2));
+      d->src[b] = dmalloc<int32_t>(d, (size_t)chunk);
+    }
+    d->bc_tid = dmalloc<double>(d, ix.n);
+    d->bc_vid = dmalloc<double>(d, ix.n);
+    d->err = dmalloc<int32_t>(d, 1);
+    CK(cudaMemsetAsync(d->err, 0, 4, st));
+    CK(cudaStreamSynchronize(st));
+  } catch (...) {
+    device_release(h);
+    throw;
+  }
+}
+
+void device_release(Handle &h) {
+  DeviceState *d = h.dev;
+  if (!d) return;
+  cudaSetDevice(d->device);
+  cudaDeviceSynchronize();
+  void *ptrs[] = {d->depth, d->send, d->arc_off, d->arc_head, d->arc_w, d->vid_of, d->tid_of, d->lab_off, d->dis,
+                  d->anc, d->ch, d->bc_tid, d->bc_vid, d->err, d->sources};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  for (int b = 0; b < 2; b++) {
+    void *q[] = {d->dc[b], d->hop[b], d->delta[b], d->order[b], d->lcnt[b], d->src[b]};
+    for (void *p : q)
+      if (p) cudaFree(p);
+    if (d->ev_label[b]) cudaEventDestroy(d->ev_label[b]);
+    if (d->ev_dep[b]) cudaEventDestroy(d->ev_dep[b]);
+  }
+  if (d->ev_start) cudaEventDestroy(d->ev_start);
+  for (auto &e : d->ev_lab) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  for (auto &e : d->ev_dp) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  if (d->s_label) cudaStreamDestroy(d->s_label);
+  if (d->s_dep) cudaStreamDestroy(d->s_dep);
+  delete d;
+  h.dev = nullptr;
+}
+
+int64_t device_bytes(const Handle &h) { return h.dev ? h.dev->bytes : 0; }
+int device_id(const Handle &h) { return h.dev ? h.dev->device : -1; }
+
+static DeviceState *need_dev(Handle &h) {
+  if (!h.dev) throw Error(QBC_EINVAL, "index is not on a device: call qbc_index_upload first");
+  CK(cudaSetDevice(h.dev->device));
+  return h.dev;
+}
+
+static void check_err(DeviceState *d) {
+  int32_t e = 0;
+  CK(cudaMemcpy(&e, d->err, 4, cudaMemcpyDeviceToHost));
+  if (e != ERR_NONE) {
+    CK(cudaMemset(d->err, 0, 4));
+    throw Error(QBC_EDEVICE, e == ERR_DISCONNECTED ? "device: SP-DAG wave pass did not reach every vertex"
+                             : e == ERR_BAD_SOURCE ? "device: source id out of range"
+                                                   : "device: kernel error word " + std::to_string(e));
+  }
+}
+
+// ------------------------------------------------------------------------------- drivers
+// Sorts nothing on the device: chunks take the source list in the given order; sources listed in
+// increasing tid order group nearby tree nodes into one CTA.
+void device_bc_sources(Handle &h, const int32_t *d_sources0, int32_t ns, double *d_bc_vid, void *stream) {
+  DeviceState *d = need_dev(h);
+  cudaStream_t user = stream ? (cudaStream_t)stream : d->s_label;
+  CK(cudaEventRecord(d->ev_start, user));
+  CK(cudaStreamWaitEvent(d->s_label, d->ev_start, 0));
+  CK(cudaStreamWaitEvent(d->s_dep, d->ev_start, 0));
+  CK(cudaMemsetAsync(d->bc_tid, 0, (size_t)d->n * 8, d->s_label));
+  CK(cudaEventRecord(d->ev_label[1], d->s_label));
+  CK(cudaStreamWaitEvent(d->s_dep, d->ev_label[1], 0));
+  int k = 0;
+  for (int32_t off = 0; off < ns; off += d->chunk, k++) {
+    const int b = k & 1;
+    const int32_t cnt = std::min(d->chunk, ns - off);
+    if (k >= 2) CK(cudaStreamWaitEvent(d->s_label, d->ev_dep[b], 0));  // buffer b free again
+    k_vid_to_tid<<<(cnt + 255) / 256, 256, 0, d->s_label>>>(d_sources0 + off, d->tid_of, d->src[b], cnt, d->n, d->err);
+    CK(cudaGetLastError());
+    d->launches++;
+    launch_label(h, d, b, cnt, false, d->s_label);
+    CK(cudaEventRecord(d->ev_label[b], d->s_label));
+    CK(cudaStreamWaitEvent(d->s_dep, d->ev_label[b], 0));
+    launch_dep(h, d, b, cnt, d->s_dep);
+    CK(cudaEventRecord(d->ev_dep[b], d->s_dep));
+  }
+  CK(cudaEventRecord(d->ev_dep[0], d->s_dep));
+  CK(cudaStreamWaitEvent(user, d->ev_dep[0], 0));
+  k_tid_to_vid_f64<<<(d->n + 255) / 256, 256, 0, user>>>(d->bc_tid, d->vid_of, d_bc_vid, d->n, 1);
+  CK(cudaGetLastError());
+  d->launches++;
+}
+
+void device_profiling(Handle &h, bool on) {
+  DeviceState *d = need_dev(h);
+  d->profiling = on;
+  d->ev_lab_used = d->ev_dp_used = 0;
+  d->label_ms = d->dep_ms = 0.0;
+  d->label_launches = d->dep_launches = d->launches = 0;
+}
+
+void device_stats(Handle &h, double *out) {
+  DeviceState *d = need_dev(h);
+  CK(cudaDeviceSynchronize());
+  for (size_t i = 0; i < d->ev_lab_used; i++) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, d->ev_lab[i].first, d->ev_lab[i].second));
+    d->label_ms += ms;
+  }
+  for (size_t i = 0; i < d->ev_dp_used; i++) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, d->ev_dp[i].first, d->ev_dp[i].second));
+    d->dep_ms += ms;
+  }
+  d->ev_lab_used = d->ev_dp_used = 0;
+  out[0] = d->label_ms;
+  out[1] = (double)d->label_launches;
+  out[2] = d->dep_ms;
+  out[3] = (double)d->dep_launches;
+  out[4] = (double)d->launches;
+}
+
+static int32_t *stage_sources(DeviceState *d, const int32_t *sources0, int32_t ns, int32_t n) {
+  for (int32_t i = 0; i < ns; i++)
+    if (sources0[i] < 0 || sources0[i] >= n) throw Error(QBC_EINVAL, "source id " + std::to_string(sources0[i]) + " out of range");
+  if (ns > d->sources_cap) {
+    if (d->sources) cudaFree(d->sources);
+    d->sources = nullptr;
+    d->sources = dmalloc<int32_t>(d, (size_t)ns);
+    d->sources_cap = ns;
+  }
+  if (ns) CK(cudaMemcpyAsync(d->sources, sources0, (size_t)ns * 4, cudaMemcpyHostToDevice, d->s_label));
+  return d->sources;
+}
+
+// host list, sorted by tid so each CTA's sources are neighbours in the tree
+static std::vector<int32_t> tid_sorted(const Index &ix, const int32_t *sources0, int32_t ns) {
+  std::vector<int32_t> v(sources0, sources0 + ns);
+  for (int32_t x : v)
+    if (x < 0 || x >= ix.n) throw Error(QBC_EINVAL, "source id " + std::to_string(x) + " out of range");
+  std::sort(v.begin(), v.end(), [&](int32_t a, int32_t b) { return ix.tid_of[a] < ix.tid_of[b]; });
+  return v;
+}
+
+void host_bc_sources(Handle &h, const int32_t *sources0, int32_t ns, double *bc_out) {
+  DeviceState *d = need_dev(h);
+  std::vector<int32_t> srt = tid_sorted(h.host, sources0, ns);
+  int32_t *ds = stage_sources(d, srt.data(), ns, d->n);
+  CK(cudaMemsetAsync(d->bc_vid, 0, (size_t)d->n * 8, d->s_label));
+  device_bc_sources(h, ds, ns, d->bc_vid, d->s_label);
+  CK(cudaMemcpyAsync(bc_out, d->bc_vid, (size_t)d->n * 8, cudaMemcpyDeviceToHost, d->s_label));
+  CK(cudaStreamSynchronize(d->s_label));
+  check_err(d);
+}
+
+void host_bc_plain(Handle &h, const int32_t *sources0, int32_t ns, double *bc_out) {
+  DeviceState *d = need_dev(h);
+  int32_t *ds = stage_sources(d, sources0, ns, d->n);
+  cudaStream_t st = d->s_label;
+  CK(cudaMemsetAsync(d->bc_tid, 0, (size_t)d->n * 8, st));
+  for (int32_t i = 0; i < ns; i++) {
+    k_vid_to_tid<<<1, 32, 0, st>>>(ds + i, d->tid_of, d->src[0], 1, d->n, d->err);
+    CK(cudaGetLastError());
+    launch_label(h, d, 0, 1, true, st);
+    launch_dep(h, d, 0, 1, st);
+  }
+  k_tid_to_vid_f64<<<(d->n + 255) / 256, 256, 0, st>>>(d->bc_tid, d->vid_of, d->bc_vid, d->n, 0);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(bc_out, d->bc_vid, (size_t)d->n * 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  check_err(d);
+}
+
+void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, uint32_t *cnt, int32_t *hop) {
+  DeviceState *d = need_dev(h);
+  cudaStream_t st = d->s_label;
+  const int32_t n = d->n;
+  int32_t *o_d = nullptr, *o_h = nullptr;
+  uint32_t *o_c = nullptr;
+  const int32_t step = std::min<int32_t>(d->chunk, 256);
+  o_d = dmalloc<int32_t>(d, (size_t)step * n);
+  if (cnt) o_c = dmalloc<uint32_t>(d, (size_t)step * n);
+  if (hop) o_h = dmalloc<int32_t>(d, (size_t)step * n);
+  try {
+    int32_t *ds = stage_sources(d, sources0, ns, n);
+    for (int32_t off = 0; off < ns; off += step) {
+      const int32_t c = std::min(step, ns - off);
+      k_vid_to_tid<<<(c + 255) / 256, 256, 0, st>>>(ds + off, d->tid_of, d->src[0], c, n, d->err);
+      CK(cudaGetLastError());
+      launch_label(h, d, 0, c, false, st);
+      if (h.host.kind == IndexKind::H2H && (cnt || hop)) {
+        // sigma and waves by the Kahn pass; BC accumulation goes to a scratch target
+        CK(cudaMemsetAsync(d->bc_tid, 0, (size_t)n * 8, st));
+        launch_dep(h, d, 0, c, st);
+      }
+      dim3 grid((n + 255) / 256, c);
+      k_rows_to_vid<<<grid, 256, 0, st>>>(d->dc[0], d->hop[0], d->vid_of, n, d->n_pad, c, o_d, o_c, o_h);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(dist + (size_t)off * n, o_d, (size_t)c * n * 4, cudaMemcpyDeviceToHost, st));
+      if (cnt) CK(cudaMemcpyAsync(cnt + (size_t)off * n, o_c, (size_t)c * n * 4, cudaMemcpyDeviceToHost, st));
+      if (hop) CK(cudaMemcpyAsync(hop + (size_t)off * n, o_h, (size_t)c * n * 4, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    }
+    check_err(d);
+  } catch (...) {
+    cudaFree(o_d); if (o_c) cudaFree(o_c); if (o_h) cudaFree(o_h);
+    throw;
+  }
+  cudaFree(o_d);
+  if (o_c) cudaFree(o_c);
+  if (o_h) cudaFree(o_h);
+  d->bytes -= (int64_t)step * n * 4 * (1 + (cnt ? 1 : 0) + (hop ? 1 : 0));
+}
+
+}  // namespace qbc

@@ -1,0 +1,47 @@
+// device.h -- device-resident index, scratch and drivers of libqbc_b200.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "host.h"
+
+namespace qbc {
+
+struct Tuning {
+  int32_t lanes_per_source = 0;  // K in {1,2,4,...,32}; sources per CTA = 32/K; 0 = auto
+  int32_t label_threads = 256;   // threads per CTA of the label kernel
+  int32_t split = 0;             // target ranges per source group; 0 = auto
+  int32_t chunk = 0;             // sources per scratch buffer; 0 = auto
+  int32_t dep_threads = 256;     // threads per CTA of the dependency kernel
+};
+
+struct DeviceState;  // opaque, defined in device.cu
+
+struct Handle {
+  Index host;
+  Tuning tuning;
+  DeviceState *dev = nullptr;
+};
+
+void device_upload(Handle &h, int device);
+void device_release(Handle &h);
+int64_t device_bytes(const Handle &h);
+int device_id(const Handle &h);  // -1 when not uploaded
+
+// BC over `sources0` (0-based vids) accumulated into d_bc_vid (n doubles, vid order, device).
+// Enqueued on `stream` (nullptr: the handle's stream); the caller synchronises.
+void device_bc_sources(Handle &h, const int32_t *d_sources0, int32_t ns, double *d_bc_vid, void *stream);
+// Same with host source list and host output (overwritten); synchronous.
+void host_bc_sources(Handle &h, const int32_t *sources0, int32_t ns, double *bc_out);
+// plain path: one source per launch pair
+void host_bc_plain(Handle &h, const int32_t *sources0, int32_t ns, double *bc_out);
+// Per-launch CUDA-event timing of the label and dependency kernels (on their own streams).
+void device_profiling(Handle &h, bool on);
+// out[0]=label ms, [1]=label launches, [2]=dependency ms, [3]=dependency launches, [4]=all launches
+// since the last device_profiling call; synchronises the device.
+void device_stats(Handle &h, double *out);
+// rows of each listed source in vid order (cnt/hop may be null)
+void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, uint32_t *cnt, int32_t *hop);
+
+}  // namespace qbc

@@ -1,0 +1,70 @@
+// host.h -- host-side types of libqbc_b200: graph, tree-decomposition index, errors.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace qbc {
+
+constexpr int32_t kInf = 999999999;  // TreeDecomp INF (src/TreeCount/TreeDecomp.h:58)
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+// Arc list as Graph::ReadGraph keeps it (src/Graph.cpp:22-36): 0-based, first duplicate kept,
+// weight 0 read as 1, arcs of each tail in file order.
+struct Graph {
+  int32_t n = 0;
+  std::vector<int32_t> off;   // n+1
+  std::vector<int32_t> head;  // arcs
+  std::vector<int32_t> w;     // arcs
+  int32_t arcs() const { return (int32_t)head.size(); }
+};
+
+// Builds the arc list from raw file lines and validates it (symmetric, simple, weights >= 1,
+// bounded total weight).  Connectivity is checked by the index builder.
+Graph graph_from_lines(int32_t n, int64_t m, const int32_t *u1, const int32_t *v1, const int32_t *w);
+Graph graph_read(const std::string &path);
+std::vector<int32_t> read_order(const std::string &path, int32_t n);
+std::vector<int32_t> read_query(const std::string &path, int32_t n);
+
+enum class IndexKind : int { MHL = 0, H2H = 1 };
+
+// Tree-decomposition index in DFS-preorder numbering ("tid").  Row p holds one entry per
+// ancestor, root first, plus the node itself last (dis 0, cnt 1, hop 0); rows start on 4-entry
+// boundaries so 16-byte vector loads stay aligned.
+struct Index {
+  IndexKind kind = IndexKind::MHL;
+  int32_t n = 0;
+  int32_t tree_height = 0, tree_width = 0;
+  std::vector<int32_t> vid_of;   // tid -> 0-based vid
+  std::vector<int32_t> tid_of;   // vid -> tid
+  std::vector<int32_t> depth;    // tid -> depth (root 1) = row length
+  std::vector<int32_t> parent;   // tid -> parent tid (-1 root)
+  std::vector<int32_t> send;     // tid -> tid + subtree size (ancestor test a <= t < send[a])
+  std::vector<int64_t> lab_off;  // n+1, entry offsets (multiples of 4)
+  std::vector<int32_t> dis;      // lab_off[n]
+  std::vector<int32_t> ch;       // 2*lab_off[n]: (cnt bits, hop) pairs; MHL only
+  std::vector<int32_t> anc;      // lab_off[n]: tid of the ancestor each row entry refers to
+  // arcs in tid space, each tail's arcs in file order
+  std::vector<int32_t> arc_off, arc_head, arc_w;
+  int64_t depth_sum = 0;
+};
+
+// TreeCount-equivalent index (distance + count + max hop) by min-degree elimination.
+Index build_mhl(const Graph &g, int nthreads);
+// H2H distance index from an order file (node_order[vid] = contraction rank).
+Index build_h2h(const Graph &g, const std::vector<int32_t> &node_order, int nthreads);
+// Min-degree contraction order (node_order[vid] = rank).
+std::vector<int32_t> min_degree_order(const Graph &g);
+
+// sum over targets of h(lca(s, t)) for each listed source (0-based vids)
+int64_t scan_entries(const Index &ix, const int32_t *sources0, int32_t ns);
+
+int hardware_threads(int requested);
+
+}  // namespace qbc

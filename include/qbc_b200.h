@@ -1,0 +1,130 @@
+/*
+ * qbc_b200.h -- C ABI of the B200-native query-based betweenness-centrality library
+ * (libqbc_b200.so).  Plain pointers and sizes only; every call returns a QBC_* status and
+ * qbc_last_error() gives the message of the calling thread's last failure.
+ *
+ * Vertex ids: file ids are 1-based (graph, query batch); every id crossing this ABI is 0-based
+ * (Graph's convention, src/Graph.cpp:24-25).  Distances are int32, shortest-path counts are the
+ * reference's 32-bit wrapping count bits (count_t = uint32_t, src/TreeCount/Util.h:24, stored in
+ * int on the device, MHLQBC.cu:94-101), hop layers int32, BC FP64 with BC(v) = 0.5 * sum_s delta_s(v)
+ * (MHLQBC.cu:469-472).
+ *
+ * Each entry point names the reference interface it replaces (paths relative to the reference).
+ */
+#ifndef QBC_B200_H
+#define QBC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  QBC_OK = 0,
+  QBC_EINVAL = 1,   /* bad argument */
+  QBC_EIO = 2,      /* file missing / malformed */
+  QBC_EGRAPH = 3,   /* graph violates an input rule (asymmetric, disconnected, weight < 1, ...) */
+  QBC_ECUDA = 4,    /* CUDA runtime error */
+  QBC_ENOMEM = 5,   /* device or host allocation refused */
+  QBC_EDEVICE = 6,  /* a kernel reported an error word (capacity exceeded, bound hit) */
+  QBC_ETIMEOUT = 7, /* served-mode wait ran out */
+  QBC_EBUSY = 8     /* served-mode admission refused (no slot / not enough free HBM) */
+};
+
+enum {
+  QBC_INDEX_MHL = 0, /* TreeCount distance + count + hop labels (MHL-QBC, RQ) */
+  QBC_INDEX_H2H = 1  /* H2H distance labels from an order file (QBC) */
+};
+
+typedef struct qbc_graph qbc_graph; /* host arc list, Graph::ReadGraph rules */
+typedef struct qbc_index qbc_index; /* host index + its device-resident copy + per-source scratch */
+
+const char *qbc_last_error(void);
+const char *qbc_version(void);
+
+/* ---- input (replaces Graph::ReadGraph, src/Graph.cpp:4-37) ----------------------------------
+ * Lines "u v w" are directed arcs, 1-based; a repeated (u,v) keeps the first arc, weight 0 reads
+ * as 1 (src/Graph.cpp:27-35).  Beyond the reference, the graph is validated: every arc needs its
+ * reverse with the same weight (the index reader symmetrises, src/TreeCount/Graph.cpp:55-71), no
+ * self loops, connected (QBC.cu:525 spins forever otherwise), and total weight < 999999999 so no
+ * distance reaches the reference's INF. */
+int qbc_graph_read(const char *path, qbc_graph **out);
+int qbc_graph_from_lines(int n, int m, const int32_t *u1, const int32_t *v1, const int32_t *w, qbc_graph **out);
+int qbc_graph_info(const qbc_graph *g, int32_t *n, int32_t *arcs);
+/* arcs in Graph's CSR order (initGraphTravel, MHLQBC.cu:130-160): off[n+1], head[arcs], w[arcs] */
+int qbc_graph_arcs(const qbc_graph *g, int32_t *off, int32_t *head, int32_t *w);
+void qbc_graph_free(qbc_graph *g);
+
+/* order file "n" + n lines "id order", 0-based ids (Graph::CHconsorderMT, src/buildIndex.cpp:6-20) */
+int qbc_read_order(const char *path, int32_t n, int32_t *node_order);
+/* query batch "q" + q 1-based ids (processBactch, RQ.cu:589-610); ids0 receives 0-based ids */
+int qbc_read_query(const char *path, int32_t n, int32_t cap, int32_t *q, int32_t *ids0);
+/* min-degree contraction order (the order-file generator Graph::GraphConstract,
+ * src/buildIndex.cpp:759-925); node_order[vid] = rank, 0 contracted first */
+int qbc_min_degree_order(const qbc_graph *g, int32_t *node_order);
+
+/* ---- index (replaces TreeDecomp Reduce/MakeTree/MakeIndex, src/TreeCount/TreeDecomp.cpp:54-511,
+ * with moveCountIndexToDevice, MHLQBC.cu:6-128; and Graph::CHconsorderMT/makeTree/makeIndex,
+ * src/buildIndex.cpp:4-310, with moveDisIndexToDevice, QBC.cu:11-127) -------------------------
+ * kind QBC_INDEX_MHL ignores node_order; QBC_INDEX_H2H requires it.  nthreads <= 0: all cores. */
+int qbc_index_build(const qbc_graph *g, int kind, const int32_t *node_order, int nthreads, qbc_index **out);
+/* copies the index to HBM of `device` (cudaSetDevice semantics, QBC.cu:601-602) */
+int qbc_index_upload(qbc_index *idx, int device);
+/* drops the device copy (keeps the host index) */
+int qbc_index_release_device(qbc_index *idx);
+/* info[0]=n, [1]=arcs, [2]=label entries, [3]=tree height, [4]=tree width, [5]=device bytes,
+ * [6]=kind, [7]=sum over vertices of depth (label bytes/12 for MHL) */
+int qbc_index_info(const qbc_index *idx, int64_t *info);
+/* Sum over the listed sources of the label entries the K2 scan reads (sum_t h(lca(s,t)));
+ * the algorithmic-bytes figure of the roofline. */
+int qbc_index_scan_entries(const qbc_index *idx, const int32_t *sources0, int32_t ns, int64_t *entries);
+void qbc_index_free(qbc_index *idx);
+/* Copies the host index out (for inspection and tests).  Arrays sized by qbc_index_info:
+ * vid_of/depth/send[n], lab_off[n+1], dis/anc[info[2]], ch[2*info[2]] (MHL only; may be NULL). */
+int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int32_t *send, int64_t *lab_off,
+                     int32_t *dis, int32_t *ch, int32_t *anc);
+
+/* Tuning of the batched path: params[0]=sources per CTA (1..32, 0=auto), [1]=threads per CTA of
+ * the label kernel, [2]=target split per source group (0=auto), [3]=sources per chunk (0=auto),
+ * [4]=threads per CTA of the dependency kernel. */
+int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams);
+int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams);
+
+/* Kernel timing: after qbc_index_profile(idx, 1) every label-scan and dependency launch is
+ * bracketed by CUDA events on its own stream; qbc_index_stats synchronises and returns
+ * out[0]=label-scan ms, [1]=label-scan launches, [2]=dependency ms, [3]=dependency launches,
+ * [4]=all kernel launches of the library since the profile call. */
+int qbc_index_profile(qbc_index *idx, int on);
+int qbc_index_stats(qbc_index *idx, double *out);
+
+/* ---- BC (replaces Graph::brandesBCIndexGPU_5, MHLQBC.cu:495-537 / QBC.cu:419-584) ------------
+ * Batched path: many sources per launch, label rows staged in shared memory, level-bucketed
+ * backprop.  bc_out: n host doubles (overwritten). */
+int qbc_bc_all(qbc_index *idx, double *bc_out);
+/* partial BC over a source list (0-based vids) */
+int qbc_bc_sources(qbc_index *idx, const int32_t *sources0, int32_t ns, double *bc_out);
+/* plain path: one source per launch sequence (label kernel, then dependency kernel) */
+int qbc_bc_plain(qbc_index *idx, const int32_t *sources0, int32_t ns, double *bc_out);
+/* Device-resident variant: d_sources0 (ns int32) and d_bc (n doubles, accumulated into, not
+ * cleared) are device pointers; stream is a cudaStream_t or NULL for the index's own stream.
+ * Returns after enqueueing; the caller synchronises. */
+int qbc_bc_sources_device(qbc_index *idx, const int32_t *d_sources0, int32_t ns, double *d_bc, void *stream);
+
+/* ---- RQ (replaces Graph::brandesBCIndexGPU_PointBatch, RQ.cu:465-531) -----------------------
+ * BC of each query vertex over all sources (the reference's pair formula equals BC restricted to
+ * the query set).  points0: q 0-based vids; out: q doubles. */
+int qbc_bc_query(qbc_index *idx, const int32_t *points0, int32_t q, double *out);
+/* many query sets sharing one source sweep: set i is points0[set_off[i] .. set_off[i+1]) */
+int qbc_bc_query_batch(qbc_index *idx, const int32_t *points0, const int32_t *set_off, int32_t nsets,
+                       const int32_t *sources0, int32_t ns, double *out);
+
+/* ---- per-source rows (the K2 output: MHLQBC.cu:334-412, RQ.cu:228-291, QBC.cu:272-331) ------
+ * dist/cnt/hop: ns*n each, row k = source sources0[k], column = 0-based vid.  cnt and hop may be
+ * NULL; for an H2H index they are filled by the device Kahn pass (QBC.cu:485-555 semantics). */
+int qbc_rows(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *dist, uint32_t *cnt, int32_t *hop);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,69 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+# the reference's real road graph: read from the reference checkout when present, else from a
+# local, uncommitted copy under tests/golden/_data/
+LA_CANDIDATES = [os.path.join(GOLDEN, "_data", "LosAngeles.txt"), "/root/reference/data/roadData/LosAngeles.txt"]
+LA_ORDER_CANDIDATES = [os.path.join(GOLDEN, "_data", "LosAngelesOrder.txt"),
+                       "/root/reference/data/orderFile/LosAngelesOrder.txt"]
+LA_QUERY_CANDIDATES = [os.path.join(GOLDEN, "_data", "LosAngelesQuery.txt"),
+                       "/root/reference/data/queryBatch/LosAngeles.txt"]
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+
+
+def _first(paths):
+    for p in paths:
+        if os.path.exists(p):
+            return p
+    return None
+
+
+@pytest.fixture(scope="session")
+def la_path():
+    p = _first(LA_CANDIDATES)
+    if p is None:
+        pytest.skip("LosAngeles graph not available")
+    return p
+
+
+@pytest.fixture(scope="session")
+def la_order_path():
+    p = _first(LA_ORDER_CANDIDATES)
+    if p is None:
+        pytest.skip("LosAngeles order file not available")
+    return p
+
+
+@pytest.fixture(scope="session")
+def la_query_path():
+    p = _first(LA_QUERY_CANDIDATES)
+    if p is None:
+        pytest.skip("LosAngeles query batch not available")
+    return p
+
+
+@pytest.fixture(scope="session")
+def g2k_path():
+    return os.path.join(GOLDEN, "g2k.txt")
+
+
+@pytest.fixture(scope="session")
+def graph_cache(tmp_path_factory):
+    return str(tmp_path_factory.mktemp("graphs"))
+
+
+def rel_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) if a.size else 0.0

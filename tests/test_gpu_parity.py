@@ -1,0 +1,221 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle and the reference's own GPU
+outputs.  Integers (dist / count bits / hop) bit-exact; BC within BC_RTOL = 1e-9 relative."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import gpu_betweennesscentrality_b200 as Q
+import pyoracle as O
+from conftest import GOLDEN, ROOT, rel_err
+from gpu_betweennesscentrality_b200 import synth
+from util import BC_RTOL, KNOWN, grid_lines, lines_of
+
+pytestmark = pytest.mark.gpu
+
+
+def _graph(n, u, v, w):
+    g = Q.Graph(device=0)
+    g.ReadLines(n, u, v, w)
+    return g
+
+
+@pytest.fixture(scope="module")
+def g2k():
+    n, u, v, w = synth.read_graph_lines(os.path.join(GOLDEN, "g2k.txt"))
+    g = _graph(n, u, v, w)
+    idx = g.build_index()
+    return n, u, v, w, g, idx, O.TreeCount(n, u, v, w), O.Arcs(n, u, v, w)
+
+
+def _order_g2k(n):
+    return Q.read_order(os.path.join(GOLDEN, "g2k.order"), n)
+
+
+def test_rows_bit_exact_all_sources_2k(g2k):
+    n, u, v, w, g, idx, tc, arcs = g2k
+    srcs = np.arange(n, dtype=np.int32)
+    d, c, h = idx.rows(srcs)
+    for s in range(0, n, 1):
+        d0, c0, h0 = tc.rows(s)
+        assert np.array_equal(d[s], d0), s
+        assert np.array_equal(c[s], c0), s
+        assert np.array_equal(h[s], h0), s
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8, 16, 32])
+def test_rows_identical_across_tunings(g2k, lanes):
+    n, u, v, w, g, idx, tc, arcs = g2k
+    srcs = np.arange(0, n, 13, dtype=np.int32)
+    base = idx.rows(srcs)
+    idx.set_tuning(lanes_per_source=lanes, label_threads=128 if lanes > 4 else 256, split=3)
+    try:
+        alt = idx.rows(srcs)
+    finally:
+        idx.set_tuning()
+    for a, b in zip(base, alt):
+        assert np.array_equal(a, b)
+
+
+def test_bc_all_2k_matches_oracle_and_reference(g2k):
+    n, u, v, w, g, idx, tc, arcs = g2k
+    bc = idx.bc_all()
+    assert rel_err(bc, tc.bc(arcs)) <= BC_RTOL
+    p = os.path.join(GOLDEN, "ref_g2k_mhl.txt")
+    if os.path.exists(p):
+        ref = np.loadtxt(p)
+        assert rel_err(bc, ref[:, 1]) <= BC_RTOL
+
+
+def test_plain_path_matches_batched(g2k):
+    n, u, v, w, g, idx, tc, arcs = g2k
+    srcs = np.arange(0, n, 9, dtype=np.int32)
+    assert rel_err(idx.bc_plain(srcs), idx.bc_sources(srcs)) <= BC_RTOL
+    assert rel_err(idx.bc_sources(srcs), tc.bc(arcs, srcs)) <= BC_RTOL
+
+
+def test_bc_repeatable_and_chunked(g2k):
+    n, u, v, w, g, idx, tc, arcs = g2k
+    a = idx.bc_all()
+    idx.set_tuning(chunk=96)
+    try:
+        b = idx.bc_all()
+    finally:
+        idx.set_tuning()
+    assert rel_err(a, b) <= BC_RTOL
+
+
+def test_qbc_h2h_2k(g2k):
+    n, u, v, w, g, idx, tc, arcs = g2k
+    order = _order_g2k(n)
+    gi = _graph(n, u, v, w)
+    hidx = gi.build_index(Q.QBC_INDEX_H2H, order)
+    h2 = O.H2H(arcs, order)
+    srcs = np.arange(0, n, 7, dtype=np.int32)
+    d, c, hop = hidx.rows(srcs)
+    for k, s in enumerate(srcs):
+        assert np.array_equal(d[k], h2.dist(int(s)))
+        d0, c0, h0 = tc.rows(int(s))
+        assert np.array_equal(c[k], c0)  # device Kahn sigma == TreeCount counts
+        assert np.array_equal(hop[k], h0)  # Kahn wave == max-hop layer
+    bc = hidx.bc_all()
+    assert rel_err(bc, h2.bc()) <= BC_RTOL
+    p = os.path.join(GOLDEN, "ref_g2k_qbc.txt")
+    if os.path.exists(p):
+        assert rel_err(bc, np.loadtxt(p)[:, 1]) <= BC_RTOL
+
+
+def test_rq_2k(g2k):
+    n, u, v, w, g, idx, tc, arcs = g2k
+    q = Q.read_query(os.path.join(GOLDEN, "g2k.query"), n)
+    out = idx.bc_query(q)
+    assert rel_err(out, tc.rq(q)) <= BC_RTOL
+    p = os.path.join(GOLDEN, "ref_g2k_rq.txt")
+    if os.path.exists(p):
+        ref = np.loadtxt(p)
+        assert np.array_equal(ref[:, 0].astype(int) - 1, q)
+        assert rel_err(out, ref[:, 1]) <= BC_RTOL
+    sets = [q[:3], q[3:], q[::-1]]
+    outs = idx.bc_query_batch(sets)
+    for s_, o_ in zip(sets, outs):
+        assert rel_err(o_, idx.bc_query(s_)) <= BC_RTOL
+
+
+@pytest.mark.parametrize("name", sorted(KNOWN))
+def test_known_graphs(name):
+    n, edges, expect = KNOWN[name]
+    nn, u, v, w = lines_of(edges, n)
+    g = _graph(nn, u, v, w)
+    idx = g.build_index()
+    bc = idx.bc_all()
+    full = O.Arcs(nn, u, v, w).bc()
+    assert rel_err(bc, full) <= BC_RTOL
+    if expect is not None:
+        assert np.allclose(bc, expect, rtol=0, atol=1e-9)
+    d, c, h = idx.rows(np.arange(n, dtype=np.int32))
+    arcs = O.Arcs(nn, u, v, w)
+    for s in range(n):
+        d0, c0, h0 = arcs.dijkstra_rows(s)
+        assert np.array_equal(d[s], d0) and np.array_equal(c[s], c0) and np.array_equal(h[s], h0)
+
+
+def test_shortcut_graph_rows_and_bc():
+    n, u, v, w = grid_lines(3000, seed=6, shortcut_frac=0.02)
+    g = _graph(n, u, v, w)
+    idx = g.build_index()
+    tc = O.TreeCount(n, u, v, w)
+    srcs = np.arange(0, n, 97, dtype=np.int32)
+    d, c, h = idx.rows(srcs)
+    for k, s in enumerate(srcs):
+        d0, c0, h0 = tc.rows(int(s))
+        assert np.array_equal(d[k], d0) and np.array_equal(c[k], c0) and np.array_equal(h[k], h0)
+    assert rel_err(idx.bc_sources(srcs), tc.bc(O.Arcs(n, u, v, w), srcs)) <= BC_RTOL
+
+
+def test_50k_sampled_rows_and_partial_bc(graph_cache):
+    path = synth.cached_graph(graph_cache, 50000, seed=1)
+    n, u, v, w = synth.read_graph_lines(path)
+    g = Q.Graph(device=0)
+    g.ReadGraph(path)
+    idx = g.build_index()
+    tc = O.TreeCount(n, u, v, w)
+    rng = np.random.default_rng(21)
+    srcs = np.sort(rng.choice(n, 48, replace=False)).astype(np.int32)
+    d, c, h = idx.rows(srcs[:12])
+    for k, s in enumerate(srcs[:12]):
+        d0, c0, h0 = tc.rows(int(s))
+        assert np.array_equal(d[k], d0) and np.array_equal(c[k], c0) and np.array_equal(h[k], h0)
+    assert rel_err(idx.bc_sources(srcs), tc.bc(O.Arcs(n, u, v, w), srcs)) <= BC_RTOL
+
+
+def test_la_full_bc_matches_reference_gpu(la_path):
+    p = os.path.join(GOLDEN, "ref_la_mhl.npz")
+    g = Q.Graph(device=0)
+    g.ReadGraph(la_path)
+    idx = g.build_index()
+    n, u, v, w = synth.read_graph_lines(la_path)
+    tc = O.TreeCount(n, u, v, w)
+    srcs = np.arange(0, n, 997, dtype=np.int32)
+    d, c, h = idx.rows(srcs)
+    for k, s in enumerate(srcs):
+        d0, c0, h0 = tc.rows(int(s))
+        assert np.array_equal(d[k], d0) and np.array_equal(c[k], c0) and np.array_equal(h[k], h0)
+    bc = idx.bc_all()
+    if os.path.exists(p):
+        assert rel_err(bc, np.load(p)["bc"]) <= BC_RTOL
+    assert rel_err(idx.bc_sources(srcs), tc.bc(O.Arcs(n, u, v, w), srcs)) <= BC_RTOL
+
+
+def test_errors_are_reported(g2k):
+    n, u, v, w, g, idx, tc, arcs = g2k
+    with pytest.raises(Q.QbcError):
+        idx.bc_sources(np.array([0, n], np.int32))
+    with pytest.raises(Q.QbcError):
+        idx.bc_query(np.array([-1], np.int32))
+    # the index is still usable afterwards
+    assert rel_err(idx.bc_sources(np.arange(5, dtype=np.int32)), tc.bc(arcs, np.arange(5, dtype=np.int32))) <= BC_RTOL
+
+
+def test_cli_drop_in(tmp_path):
+    g = os.path.join(GOLDEN, "g2k.txt")
+    binp = os.path.join(ROOT, "gpu_betweennesscentrality_b200", "bin")
+    env = dict(os.environ, QBC_OUTPUT_DIGITS="17")
+    r = subprocess.run([os.path.join(binp, "MHLQBC"), g, "0", str(tmp_path / "mhl.txt")], capture_output=True,
+                       text=True, env=env, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "seconds (---totalTime---)" in r.stdout and r.stdout.startswith("roadDataPath:")
+    out = np.loadtxt(tmp_path / "mhl.txt", skiprows=1)
+    n, u, vv, w = synth.read_graph_lines(g)
+    ref = O.TreeCount(n, u, vv, w).bc(O.Arcs(n, u, vv, w))
+    assert rel_err(out[:, 1], ref) <= BC_RTOL
+    std = tmp_path / "std.txt"  # standard-BC file format of QBC.cu:632-638: "n m" then "vid bc"
+    std.write_text(f"{n} {u.shape[0]}\n" + "".join(f"{i + 1} {x:.17g}\n" for i, x in enumerate(ref)))
+    r = subprocess.run([os.path.join(binp, "QBC"), g, os.path.join(GOLDEN, "g2k.order"), "0", str(tmp_path / "q.txt"),
+                        str(std)], capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "BC value is correct" in r.stdout
+    r = subprocess.run([os.path.join(binp, "RQ"), g, os.path.join(GOLDEN, "g2k.query"), "0"], capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "The number of vertices to query: 10" in r.stdout and "vertexID" in r.stdout

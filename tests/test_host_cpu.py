@@ -1,0 +1,206 @@
+"""CPU: the C-ABI library loads and exports every declared symbol; readers, input validation and
+the host-side index builders (checked against the oracle with a numpy restatement of the scan)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import gpu_betweennesscentrality_b200 as Q
+import pyoracle as O
+from conftest import GOLDEN, ROOT
+from gpu_betweennesscentrality_b200 import capi, synth
+from util import KNOWN, grid_lines, lines_of
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "qbc_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(qbc_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = capi.lib()
+    names = declared_symbols()
+    assert len(names) >= 25
+    for name in names:
+        assert hasattr(L, name), name
+        assert name in capi.SIGNATURES, f"{name} has no ctypes signature"
+    assert b"sm_100a" in L.qbc_version()
+
+
+def test_cli_binaries_built():
+    for b in ["MHLQBC", "QBC", "RQ"]:
+        assert os.access(os.path.join(ROOT, "gpu_betweennesscentrality_b200", "bin", b), os.X_OK)
+
+
+# ------------------------------------------------------------------------------------ readers
+def test_reader_keeps_first_duplicate_and_maps_zero_weight(tmp_path):
+    p = tmp_path / "g.txt"
+    # arcs (1-based): 1->2 w0 (reads 1), duplicate 1->2 w1, reverse 2->1 w1, 2->3/3->2 w5
+    p.write_text("3 5\n1 2 0\n1 2 1\n2 1 1\n2 3 5\n3 2 5\n")
+    g = Q.Graph()
+    g.ReadGraph(str(p))
+    off, head, w = g.arcs()
+    assert g.nodenum == 3 and g.edgenum == 4
+    assert off.tolist() == [0, 1, 3, 4] and head.tolist() == [1, 0, 2, 1] and w.tolist() == [1, 1, 5, 5]
+
+
+@pytest.mark.parametrize("text,code", [
+    ("3 2\n1 2 4\n2 3 4\n", capi.QBC_EGRAPH),                  # no reverse arcs
+    ("2 2\n1 2 4\n2 1 5\n", capi.QBC_EGRAPH),                  # weights differ
+    ("2 2\n1 1 4\n1 1 4\n", capi.QBC_EGRAPH),                  # self loop
+    ("2 2\n1 3 4\n3 1 4\n", capi.QBC_EIO),                     # id out of range
+    ("2 4\n1 2 4\n2 1 4\n", capi.QBC_EIO),                     # truncated
+    ("2 4\n1 2 4\n2 1 4\n1 2 6\n2 1 6\n", capi.QBC_EGRAPH),    # duplicate with another weight
+    ("2 2\n1 2 -3\n2 1 -3\n", capi.QBC_EGRAPH),                # negative weight
+])
+def test_reader_rejects(tmp_path, text, code):
+    p = tmp_path / "bad.txt"
+    p.write_text(text)
+    with pytest.raises(Q.QbcError) as e:
+        Q.Graph().ReadGraph(str(p))
+    assert e.value.code == code
+
+
+def test_missing_file():
+    with pytest.raises(Q.QbcError) as e:
+        Q.Graph().ReadGraph("/nonexistent/graph.txt")
+    assert e.value.code == capi.QBC_EIO
+
+
+def test_disconnected_graph_rejected_by_index_build():
+    n, u, v, w = lines_of([(0, 1, 1), (2, 3, 1)], 4)
+    g = Q.Graph()
+    g.ReadLines(n, u, v, w)
+    with pytest.raises(Q.QbcError) as e:
+        g.build_index(upload=False)
+    assert e.value.code == capi.QBC_EGRAPH and "connected" in str(e.value)
+
+
+def test_order_and_query_readers(tmp_path):
+    n = 2024
+    o = Q.read_order(os.path.join(GOLDEN, "g2k.order"), n)
+    assert sorted(o.tolist()) == list(range(n))
+    qids = Q.read_query(os.path.join(GOLDEN, "g2k.query"), n)
+    assert qids.shape == (10,) and qids.min() >= 0 and qids.max() < n
+    bad = tmp_path / "o.txt"
+    bad.write_text("3\n0 0\n1 0\n2 1\n")
+    with pytest.raises(Q.QbcError):
+        Q.read_order(str(bad), 3)
+    bq = tmp_path / "q.txt"
+    bq.write_text("3\n1\n2\n")
+    with pytest.raises(Q.QbcError):
+        Q.read_query(str(bq), 3)
+
+
+def test_reference_query_batches_readable(la_query_path, la_path):
+    n, _, _, _ = synth.read_graph_lines(la_path)
+    ids = Q.read_query(la_query_path, n)
+    assert ids.shape[0] == 10
+
+
+# ------------------------------------------------------------------------------- host index
+def scan_rows(ex, sources_vid):
+    """numpy restatement of the K1+K2 scan over the exported index (self-inclusive rows)."""
+    n = ex["vid_of"].shape[0]
+    H = int(ex["depth"].max())
+    A = np.full((n, H), -1, np.int64)
+    D = np.full((n, H), 10 ** 12, np.int64)
+    C = np.zeros((n, H), np.uint64)
+    HP = np.zeros((n, H), np.int64)
+    for t in range(n):
+        o, h = ex["lab_off"][t], ex["depth"][t]
+        A[t, :h] = ex["anc"][o:o + h]
+        D[t, :h] = ex["dis"][o:o + h]
+        if ex["ch"] is not None:
+            C[t, :h] = ex["ch"][2 * o:2 * o + 2 * h:2].astype(np.uint32)
+            HP[t, :h] = ex["ch"][2 * o + 1:2 * o + 2 * h:2]
+    tid_of = np.empty(n, np.int64)
+    tid_of[ex["vid_of"]] = np.arange(n)
+    out = []
+    for s in sources_vid:
+        ts = tid_of[s]
+        lcad = np.cumprod(A == A[ts][None, :], axis=1).sum(1)
+        S = np.where(np.arange(H)[None, :] < lcad[:, None], D + D[ts][None, :], 1 << 50)
+        m = S.min(1)
+        eq = S == m[:, None]
+        c = (((C * C[ts][None, :]) % (1 << 32)) * eq).sum(1) % (1 << 32)
+        hh = np.where(eq, HP + HP[ts][None, :], -1).max(1)
+        out.append((m[tid_of].astype(np.int64), c[tid_of].astype(np.uint32), hh[tid_of]))
+    return out
+
+
+@pytest.mark.parametrize("n_target,seed,sc", [(2000, 1, 0.0), (900, 5, 0.02), (300, 8, 0.05)])
+def test_mhl_index_rows_match_oracle(n_target, seed, sc):
+    n, u, v, w = grid_lines(n_target, seed=seed, shortcut_frac=sc)
+    g = Q.Graph(nthreads=4)
+    g.ReadLines(n, u, v, w)
+    idx = g.build_index(upload=False)
+    ex = idx.export()
+    tc = O.TreeCount(n, u, v, w)
+    srcs = [0, n // 3, n - 1]
+    for s, (d, c, h) in zip(srcs, scan_rows(ex, srcs)):
+        d0, c0, h0 = tc.rows(s)
+        assert np.array_equal(d, d0) and np.array_equal(c, c0) and np.array_equal(h, h0)
+
+
+@pytest.mark.parametrize("name", sorted(KNOWN))
+def test_known_graph_index_rows(name):
+    n, edges, _ = KNOWN[name]
+    nn, u, v, w = lines_of(edges, n)
+    g = Q.Graph()
+    g.ReadLines(nn, u, v, w)
+    idx = g.build_index(upload=False)
+    ex = idx.export()
+    arcs = O.Arcs(nn, u, v, w)
+    for s, (d, c, h) in zip(range(n), scan_rows(ex, list(range(n)))):
+        d0, c0, h0 = arcs.dijkstra_rows(s)
+        assert np.array_equal(d, d0) and np.array_equal(c, c0) and np.array_equal(h, h0)
+
+
+def test_h2h_index_rows_are_true_distances():
+    n, u, v, w = synth.read_graph_lines(os.path.join(GOLDEN, "g2k.txt"))
+    order = Q.read_order(os.path.join(GOLDEN, "g2k.order"), n)
+    g = Q.Graph()
+    g.ReadLines(n, u, v, w)
+    idx = g.build_index(Q.QBC_INDEX_H2H, order, upload=False)
+    ex = idx.export()
+    arcs = O.Arcs(n, u, v, w)
+    rng = np.random.default_rng(1)
+    for t in rng.choice(n, 25, replace=False):
+        d0, _, _ = arcs.dijkstra_rows(int(ex["vid_of"][t]))
+        o, h = ex["lab_off"][t], ex["depth"][t]
+        anc_vid = ex["vid_of"][ex["anc"][o:o + h]]
+        assert np.array_equal(ex["dis"][o:o + h], d0[anc_vid])
+    # same tree as the reference's H2H for the same order (heights multiset)
+    h2 = O.H2H(arcs, order)
+    assert sorted(ex["depth"].tolist()) == sorted(h2.height.tolist())
+
+
+def test_min_degree_order_is_permutation():
+    n, u, v, w = grid_lines(500, seed=2)
+    g = Q.Graph()
+    g.ReadLines(n, u, v, w)
+    o = g.min_degree_order()
+    assert sorted(o.tolist()) == list(range(n))
+
+
+def test_scan_entries_matches_lca_depth_sum():
+    n, u, v, w = grid_lines(400, seed=3)
+    g = Q.Graph()
+    g.ReadLines(n, u, v, w)
+    idx = g.build_index(upload=False)
+    ex = idx.export()
+    H = int(ex["depth"].max())
+    A = np.full((n, H), -1, np.int64)
+    for t in range(n):
+        o, h = ex["lab_off"][t], ex["depth"][t]
+        A[t, :h] = ex["anc"][o:o + h]
+    tid_of = np.empty(n, np.int64)
+    tid_of[ex["vid_of"]] = np.arange(n)
+    srcs = [0, 17, 399]
+    # common-prefix length of the ancestor rows, capped at the row length (padding compares equal)
+    want = sum(int(np.minimum(np.cumprod(A == A[tid_of[s]][None, :], axis=1).sum(1), ex["depth"]).sum())
+               for s in srcs)
+    assert idx.scan_entries(srcs) == want
