@@ -38,6 +38,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--la", default=None)
     a = ap.parse_args()
+    if a.la:
+        a.la = os.path.abspath(a.la)
     g = os.path.join(HERE, "g2k.txt")
     timings = {}
     timings["g2k_mhl"] = run("ref_mhlqbc", [g], os.path.join(HERE, "ref_g2k_mhl.txt"))
