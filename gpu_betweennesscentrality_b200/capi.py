@@ -52,6 +52,7 @@ SIGNATURES = {
     "qbc_bc_query_batch": (C.c_int, [vp, i32p, i32p, C.c_int32, i32p, C.c_int32, f64p]),
     "qbc_index_profile": (C.c_int, [vp, C.c_int]),
     "qbc_index_stats": (C.c_int, [vp, f64p]),
+    "qbc_bc_source_static": (C.c_int, [vp, C.c_int32, vp, vp]),
     "qbc_rows": (C.c_int, [vp, i32p, C.c_int32, i32p, u32p, i32p]),
 }
 

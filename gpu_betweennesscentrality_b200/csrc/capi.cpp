@@ -290,6 +290,13 @@ int qbc_index_stats(qbc_index *idx, double *out) {
   });
 }
 
+int qbc_bc_source_static(qbc_index *idx, int32_t source0, double *d_bc, void *stream) {
+  return guarded([&] {
+    need(idx, "null index");
+    qbc::host_bc_source_static(idx->h, source0, d_bc, stream);
+  });
+}
+
 int qbc_rows(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *dist, uint32_t *cnt, int32_t *hop) {
   return guarded([&] {
     need(idx && dist && ns >= 0 && (ns == 0 || sources0), "null argument");

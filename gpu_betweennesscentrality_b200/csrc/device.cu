@@ -26,7 +26,9 @@
 #include <climits>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/qbc_b200.h"
 #include "device.h"
@@ -953,4 +955,109 @@ void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, ui
   d->bytes -= (int64_t)step * n * 4 * (1 + (cnt ? 1 : 0) + (hop ? 1 : 0));
 }
 
+// ------------------------------------------------------------------ allocation-free single source
+// qbc_bc_source_static: one source's BC contribution without any device allocation in the call.
+// Some callers cannot allocate device memory at the point where they need BC: a host application
+// whose memory manager has already reserved the GPU's memory (a framework's caching allocator),
+// or a serving loop whose steady state must stay free of cudaMalloc/cudaFree because those calls
+// synchronise the device and have unbounded latency.  For them the per-source scratch (distance /
+// sigma pairs, hop layers, dependencies, level queue, layer counters, a BC accumulator) lives in
+// this statically sized device array instead of the index's allocated scratch buffers.  Every GPU
+// that loads the library holds it (kStaticScratchBytes, about 5 MiB) until the process exits.
+constexpr int32_t kStaticMaxVertices = 1 << 17;  // largest graph the static scratch serves
+constexpr size_t kStaticDc = 0;                                                     // int2[max]
+constexpr size_t kStaticHop = kStaticDc + (size_t)kStaticMaxVertices * 8;           // int32[max]
+constexpr size_t kStaticDelta = kStaticHop + (size_t)kStaticMaxVertices * 4;        // double[max]
+constexpr size_t kStaticOrder = kStaticDelta + (size_t)kStaticMaxVertices * 8;      // int32[max]
+constexpr size_t kStaticLcnt = kStaticOrder + (size_t)kStaticMaxVertices * 4;       // int32[2*(max+2)]
+constexpr size_t kStaticBc = kStaticLcnt + (((size_t)2 * (kStaticMaxVertices + 2) * 4 + 255) / 256) * 256;  // double[max]
+constexpr size_t kStaticSrc = kStaticBc + (size_t)kStaticMaxVertices * 8;           // int32[64]
+constexpr size_t kStaticScratchBytes = kStaticSrc + 256;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+__global__ void k_static_set_source(int32_t *dst, int32_t tid) { *dst = tid; }
+
+// Address of g_static_scratch on `device`.  The symbol name is only a host-side stand-in, so
+// the device address is looked up once per device with that device current, and cached.
+static unsigned char *static_scratch_on(int device) {
+  static std::mutex mu;
+  static std::vector<unsigned char *> cached;
+  std::lock_guard<std::mutex> lock(mu);
+  if (device < 0) throw Error(QBC_EINVAL, "bad device");
+  if ((size_t)device >= cached.size()) cached.resize((size_t)device + 1, nullptr);
+  if (!cached[device]) {
+    int cur = -1;
+    CK(cudaGetDevice(&cur));
+    if (cur != device) throw Error(QBC_EINVAL, "static scratch set-up needs the index's device current");
+    void *ptr = nullptr;
+    CK(cudaGetSymbolAddress(&ptr, g_static_scratch));
+    cached[device] = (unsigned char *)ptr;
+  }
+  return cached[device];
+}
+
+void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *stream) {
+  if (h.host.n > kStaticMaxVertices)
+    throw Error(QBC_EINVAL, "graph has " + std::to_string(h.host.n) + " vertices; the static-scratch entry point serves at most " +
+                                std::to_string(kStaticMaxVertices));
+  if (source0 < 0 || source0 >= h.host.n) throw Error(QBC_EINVAL, "source id " + std::to_string(source0) + " out of range");
+  if (!d_bc_vid) throw Error(QBC_EINVAL, "null BC output");
+  DeviceState *d = need_dev(h);
+  unsigned char *base = static_scratch_on(d->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : d->s_label;
+  int2 *dc = reinterpret_cast<int2 *>(base + kStaticDc);
+  int32_t *hop = reinterpret_cast<int32_t *>(base + kStaticHop);
+  double *delta = reinterpret_cast<double *>(base + kStaticDelta);
+  int32_t *order = reinterpret_cast<int32_t *>(base + kStaticOrder);
+  int32_t *lcnt = reinterpret_cast<int32_t *>(base + kStaticLcnt);
+  double *bc_tid = reinterpret_cast<double *>(base + kStaticBc);
+  int32_t *src = reinterpret_cast<int32_t *>(base + kStaticSrc);
+  // the array keeps the previous call's contents: the BC accumulator must start at zero; every
+  // other region is fully written by the kernels before it is read
+  CK(cudaMemsetAsync(bc_tid, 0, (size_t)d->n * 8, st));
+  k_static_set_source<<<1, 1, 0, st>>>(src, h.host.tid_of[source0]);
+  CK(cudaGetLastError());
+  const LabelPlan p = plan_label(h, d, 1, true);
+  LabelArgs la{};
+  la.dis = d->dis;
+  la.ch = d->ch;
+  la.anc = d->anc;
+  la.lab_off = d->lab_off;
+  la.depth = d->depth;
+  la.send = d->send;
+  la.src = src;
+  la.ns = 1;
+  la.n = d->n;
+  la.n_pad = d->n_pad;
+  la.stride = p.S;
+  la.split = p.split;
+  la.out_dc = dc;
+  la.out_hop = hop;
+  if (h.host.kind == IndexKind::MHL) launch_label_c<true>(p, la, 1, st);
+  else launch_label_c<false>(p, la, 1, st);
+  DepArgs da{};
+  da.arc_off = d->arc_off;
+  da.arc_head = d->arc_head;
+  da.arc_w = d->arc_w;
+  da.src = src;
+  da.ns = 1;
+  da.n = d->n;
+  da.n_pad = d->n_pad;
+  da.dc = dc;
+  da.hop = hop;
+  da.delta = delta;
+  da.order = order;
+  da.lcnt = lcnt;
+  da.bc = bc_tid;
+  da.err = d->err;
+  const int threads = std::max(64, std::min(256, (h.tuning.dep_threads / 32) * 32));
+  if (h.host.kind == IndexKind::MHL) k_dependency<<<1, threads, 0, st>>>(da);
+  else k_kahn_dependency<<<1, threads, 0, st>>>(da);
+  CK(cudaGetLastError());
+  k_tid_to_vid_f64<<<(d->n + 255) / 256, 256, 0, st>>>(bc_tid, d->vid_of, d_bc_vid, d->n, 1);
+  CK(cudaGetLastError());
+}
+
 }  // namespace qbc
+

@@ -44,4 +44,8 @@ void device_stats(Handle &h, double *out);
 // rows of each listed source in vid order (cnt/hop may be null)
 void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, uint32_t *cnt, int32_t *hop);
 
+// One source's BC contribution added into d_bc_vid (device, n doubles, vid order) using only the
+// library's static device scratch; enqueued on `stream` (nullptr: the index's stream).
+void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *stream);
+
 }  // namespace qbc

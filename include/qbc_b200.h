@@ -111,6 +111,21 @@ int qbc_bc_plain(qbc_index *idx, const int32_t *sources0, int32_t ns, double *bc
  * Returns after enqueueing; the caller synchronises. */
 int qbc_bc_sources_device(qbc_index *idx, const int32_t *d_sources0, int32_t ns, double *d_bc, void *stream);
 
+/* One source's BC contribution without allocating: no counterpart in the reference.
+ * For callers that cannot allocate device memory when they need BC -- a host application whose
+ * memory manager already holds the GPU's memory, or a serving loop that must stay free of
+ * cudaMalloc/cudaFree (they synchronise the device and have unbounded latency).  The per-source
+ * scratch lives in a static device array built into the library (about 5 MiB, held by every GPU
+ * that loads the library until the process exits), so graphs are limited to
+ * QBC_STATIC_MAX_VERTICES vertices (larger ones return QBC_EINVAL).  The index must already be
+ * uploaded.  Adds 0.5*delta_s(v) into d_bc (device pointer, n doubles, 0-based vid order) on
+ * `stream` (NULL: the index's stream); the caller synchronises.  The first call on a device looks
+ * up the array's device address with that device current; make that first call before any stream
+ * capture.  All calls share the one array, which keeps the previous call's contents: calls that
+ * overlap on the GPU (other streams, other host threads) race, so issue them in one stream. */
+#define QBC_STATIC_MAX_VERTICES 131072
+int qbc_bc_source_static(qbc_index *idx, int32_t source0, double *d_bc, void *stream);
+
 /* ---- RQ (replaces Graph::brandesBCIndexGPU_PointBatch, RQ.cu:465-531) -----------------------
  * BC of each query vertex over all sources (the reference's pair formula equals BC restricted to
  * the query set).  points0: q 0-based vids; out: q doubles. */
