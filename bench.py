@@ -176,6 +176,7 @@ def main():
     ap.add_argument("--n", type=int, default=50000)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--chunk", type=int, default=0, help="sources per scratch buffer (0: sized from free HBM)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -210,6 +211,8 @@ def main():
     t = time.perf_counter()
     idx = G.build_index(upload=False)
     t_build = time.perf_counter() - t
+    if args.chunk:
+        idx.set_tuning(chunk=args.chunk)
     t = time.perf_counter()
     idx.upload(local)
     torch.cuda.synchronize()

@@ -123,14 +123,16 @@ class Index:
         check(lib().qbc_index_scan_entries(self.h, ptr(s, i32p), int(s.shape[0]), C.byref(e)))
         return int(e.value)
 
-    def set_tuning(self, lanes_per_source=0, label_threads=256, split=0, chunk=0, dep_threads=256):
-        p = i32([lanes_per_source, label_threads, split, chunk, dep_threads])
-        check(lib().qbc_index_set_tuning(self.h, ptr(p, i32p), 5))
+    TUNING_KEYS = ("lanes_per_source", "label_threads", "split", "chunk", "dep_threads", "dep_form")
+
+    def set_tuning(self, lanes_per_source=0, label_threads=256, split=0, chunk=0, dep_threads=256, dep_form=0):
+        p = i32([lanes_per_source, label_threads, split, chunk, dep_threads, dep_form])
+        check(lib().qbc_index_set_tuning(self.h, ptr(p, i32p), 6))
 
     def get_tuning(self):
-        p = np.zeros(5, np.int32)
-        check(lib().qbc_index_get_tuning(self.h, ptr(p, i32p), 5))
-        return dict(zip(["lanes_per_source", "label_threads", "split", "chunk", "dep_threads"], p.tolist()))
+        p = np.zeros(6, np.int32)
+        check(lib().qbc_index_get_tuning(self.h, ptr(p, i32p), 6))
+        return dict(zip(self.TUNING_KEYS, p.tolist()))
 
     def profile(self, on: bool = True) -> None:
         check(lib().qbc_index_profile(self.h, 1 if on else 0))

@@ -191,13 +191,14 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
   return guarded([&] {
     need(idx && (nparams == 0 || params), "null argument");
     qbc::Tuning &t = idx->h.tuning;
-    int32_t *f[] = {&t.lanes_per_source, &t.label_threads, &t.split, &t.chunk, &t.dep_threads};
+    int32_t *f[] = {&t.lanes_per_source, &t.label_threads, &t.split, &t.chunk, &t.dep_threads, &t.dep_form};
     if (nparams > 0) {
       int32_t k = params[0];
       need(k == 0 || k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32, "lanes per source must be 0 or a power of two <= 32");
     }
     const int32_t old_chunk = t.chunk;
-    for (int32_t i = 0; i < nparams && i < 5; i++) *f[i] = params[i];
+    if (nparams > 5) need(params[5] >= 0 && params[5] <= 2, "dependency form must be 0, 1 or 2");
+    for (int32_t i = 0; i < nparams && i < 6; i++) *f[i] = params[i];
     if (nparams > 3 && t.chunk != old_chunk && idx->h.dev) qbc::device_upload(idx->h, qbc::device_id(idx->h));
   });
 }
@@ -206,8 +207,8 @@ int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams)
   return guarded([&] {
     need(idx && (nparams == 0 || params), "null argument");
     const qbc::Tuning &t = idx->h.tuning;
-    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads};
-    for (int32_t i = 0; i < nparams && i < 5; i++) params[i] = f[i];
+    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form};
+    for (int32_t i = 0; i < nparams && i < 6; i++) params[i] = f[i];
   });
 }
 

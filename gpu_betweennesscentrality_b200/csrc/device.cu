@@ -18,8 +18,9 @@
 //   k_kahn_dependency (QBC) distance-only rows from the H2H index; sigma and topological waves
 //                  by a device Kahn pass (QBC.cu:485-555 ran it on the host), then the same backprop.
 //
-// Chunks of sources are double-buffered over two streams so the compute-bound label scan of chunk
-// k+1 overlaps the latency-bound dependency pass of chunk k.
+// Chunks of sources alternate between two scratch buffers; the label scan and the dependency pass
+// of a chunk run back to back on one stream (concurrent on two streams they thrash each other's
+// caches: measured ~2x slower in total).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -43,10 +44,25 @@ namespace qbc {
                   std::string(#call) + ": " + cudaGetErrorString(e_));                              \
   } while (0)
 
-enum : int32_t { ERR_NONE = 0, ERR_HOP_CAP = 1, ERR_DISCONNECTED = 2, ERR_BAD_SOURCE = 3 };
+enum : int32_t { ERR_NONE = 0, ERR_HOP_CAP = 1, ERR_DISCONNECTED = 2, ERR_BAD_SOURCE = 3, ERR_COPY_TIMEOUT = 4 };
 
 constexpr int kLayerCap = 4094;  // shared-memory layer counters; deeper DAGs use global memory
 constexpr unsigned kFull = 0xffffffffu;
+
+// Per-source rows (dist/sigma pairs, hop layers) of a buffer with ns source slots are stored
+// chunk-blocked: entry (slot, t) lives at ((t / 8) * ns + slot) * 8 + t % 8, so the 8-target
+// chunk of the 32 consecutive slots a warp produces is one contiguous block.  With ns = 1 this is
+// the plain row layout.
+__host__ __device__ __forceinline__ size_t blk(int slot, int t, int ns) {
+  return ((size_t)(t >> 3) * (size_t)ns + (size_t)slot) * 8 + (size_t)(t & 7);
+}
+
+template <class T>
+struct RowView {
+  T *p;
+  int slot, ns;
+  __device__ __forceinline__ T &operator[](int t) const { return p[blk(slot, t, ns)]; }
+};
 
 // ------------------------------------------------------------------------------- state
 struct DeviceState {
@@ -55,7 +71,9 @@ struct DeviceState {
   cudaEvent_t ev_label[2] = {nullptr, nullptr}, ev_dep[2] = {nullptr, nullptr}, ev_start = nullptr;
   int32_t n = 0, n_pad = 0, hmax_pad = 0;
   int32_t *depth = nullptr, *send = nullptr, *arc_off = nullptr, *arc_head = nullptr, *arc_w = nullptr;
-  int32_t *vid_of = nullptr, *tid_of = nullptr, *dis = nullptr, *anc = nullptr;
+  int2 *arc_rng = nullptr, *arc_hw = nullptr;
+  int32_t *vid_of = nullptr, *tid_of = nullptr, *dis = nullptr, *anc = nullptr, *aend = nullptr;
+  int32_t packed_bits = 0;  // > 0: the packed-key label scan applies
   int64_t *lab_off = nullptr;
   int2 *ch = nullptr;
   // scratch, two buffers of `chunk` slots
@@ -66,6 +84,7 @@ struct DeviceState {
   int32_t *order[2] = {nullptr, nullptr};
   int32_t *lcnt[2] = {nullptr, nullptr};
   int32_t *src[2] = {nullptr, nullptr};
+  int32_t *maxhop[2] = {nullptr, nullptr};
   double *bc_tid = nullptr;
   double *bc_vid = nullptr;
   int32_t *sources = nullptr;  // staging for host source lists
@@ -120,6 +139,10 @@ struct LabelArgs {
   int32_t ns, n, n_pad, stride, split;
   int2 *__restrict__ out_dc;      // [ns][n_pad] (dist, count bits)
   int32_t *__restrict__ out_hop;  // [ns][n_pad]
+  int32_t *__restrict__ maxhop;   // [ns] largest hop layer per source (atomicMax), or null
+  const int32_t *__restrict__ aend;  // subtree end of each row entry's ancestor (packed kernel)
+  int32_t bits;                      // index bits of the packed keys (packed kernel)
+  int32_t *err;                      // device error word (packed kernel's bounded waits)
 };
 
 // largest J with lo[J] <= t < hi[J] (entry 0 is the root and always holds), returned as J+1
@@ -278,13 +301,19 @@ __global__ void __launch_bounds__(256, 1) k_label_scan(LabelArgs a) {
     }
     if (have && kq == 0) {
       const size_t slot = (size_t)(first + si);
-      int4 *od = reinterpret_cast<int4 *>(a.out_dc + slot * a.n_pad + t0);
+      if (COUNTS && a.maxhop) {
+        int mh = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) mh = max(mh, rh[k]);
+        atomicMax(a.maxhop + slot, mh);
+      }
+      int4 *od = reinterpret_cast<int4 *>(a.out_dc + blk((int)slot, t0, a.ns));
       od[0] = make_int4(rd[0], rc[0], rd[1], rc[1]);
       od[1] = make_int4(rd[2], rc[2], rd[3], rc[3]);
       od[2] = make_int4(rd[4], rc[4], rd[5], rc[5]);
       od[3] = make_int4(rd[6], rc[6], rd[7], rc[7]);
       if (COUNTS) {
-        int4 *oh = reinterpret_cast<int4 *>(a.out_hop + slot * a.n_pad + t0);
+        int4 *oh = reinterpret_cast<int4 *>(a.out_hop + blk((int)slot, t0, a.ns));
         oh[0] = make_int4(rh[0], rh[1], rh[2], rh[3]);
         oh[1] = make_int4(rh[4], rh[5], rh[6], rh[7]);
       }
@@ -292,8 +321,272 @@ __global__ void __launch_bounds__(256, 1) k_label_scan(LabelArgs a) {
   }
 }
 
+// Packed-key label scan (K=1, 32 sources per CTA).  Each source entry is stored as the key
+// (dist << B) | j and each target entry is shifted by B on the fly, so one shift-add gives
+// (d_s+d_t, j) and a running unsigned min yields the distance and the smallest minimising j at
+// once; a second min over key ^ (2^B-1) yields the largest minimising j, so a tie exists iff the two
+// differ.  Valid when every row has at most 2^B entries and 2*max_label < 2^(32-B) - 1 (checked
+// on the host).  Target rows arrive by 1-D TMA bulk copies (cp.async.bulk, no multicast) into two
+// per-warp shared buffers, the row of the next target in flight while the current one is scanned;
+// ancestor intervals come from the L1-cached global rows anc/aend.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void bulk_row_to_smem(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+// bounded wait for the phase with the given parity; false when the bound ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  for (uint32_t it = 0; it < (1u << 22); it++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+constexpr int kPackedThreads = 512;
+constexpr int kPackedWarps = kPackedThreads / 32;
+constexpr int kRowBuffers = 2;  // per-warp target-row buffers: 1 copy in flight
+constexpr int kStageInt4 = 32 * 5 + 32 * 3;  // per-warp output staging (int4s)
+
+template <bool COUNTS>
+__global__ void __launch_bounds__(kPackedThreads, 1) k_label_scan_packed(LabelArgs a) {
+  constexpr int G = 32;
+  extern __shared__ int4 smem4[];
+  uint32_t *s_key = reinterpret_cast<uint32_t *>(smem4);
+  const int S = a.stride;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  int32_t *tb0 = reinterpret_cast<int32_t *>(s_key + G * S) + warp * kRowBuffers * S;
+  int4 *sdc = reinterpret_cast<int4 *>(s_key + G * S + nwarps * kRowBuffers * S) + warp * kStageInt4;
+  int4 *shp = sdc + 32 * 5;
+  int2 *sdc2 = reinterpret_cast<int2 *>(sdc) + lane * 10;  // this lane's 8 (dist, count) pairs
+  int32_t *shp1 = reinterpret_cast<int32_t *>(shp) + lane * 12;  // this lane's 8 hop layers
+  __shared__ int32_t s_h[G];
+  __shared__ int64_t s_off[G];
+  __shared__ __align__(8) uint64_t s_bar[kPackedWarps][kRowBuffers];
+  const int first = blockIdx.y * G;
+  if (first >= a.ns) return;
+  const int gcount = min(G, a.ns - first);
+  const uint32_t B = (uint32_t)a.bits, mask = (1u << B) - 1u;
+  if (threadIdx.x < G) {
+    const int i = threadIdx.x;
+    const int s = i < gcount ? a.src[first + i] : 0;
+    s_h[i] = i < gcount ? a.depth[s] : 0;
+    s_off[i] = a.lab_off[s];
+  }
+  if (lane == 0)
+    for (int b = 0; b < kRowBuffers; b++) mbar_init(&s_bar[warp][b], 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < G * S; idx += blockDim.x) {
+    const int i = idx / S, j = idx - i * S;
+    uint32_t key = 0xffffffffu;
+    if (i < gcount && j < s_h[i]) key = ((uint32_t)a.dis[s_off[i] + j] << B) | (uint32_t)j;
+    s_key[idx] = key;
+  }
+  __syncthreads();
+
+  const bool have = lane < gcount;
+  const int hs = have ? s_h[lane] : 1;
+  const int64_t soff = s_off[lane];
+  const uint32_t *srow = s_key + lane * S;
+  const int32_t *lo = a.anc + soff;
+  const int32_t *hi = a.aend + soff;
+  const int nsteps = 32 - __clz(hs);
+  int mh = 0;
+  bool failed = false;
+
+  const int nchunk = a.n_pad >> 3;
+  const int cbeg = (int)((int64_t)nchunk * blockIdx.x / a.split);
+  const int cend = (int)((int64_t)nchunk * (blockIdx.x + 1) / a.split);
+  uint32_t issued = 0, done = 0;
+  int next_c = cbeg + warp, next_k = 0;
+  auto issue_next = [&]() {
+    if (next_c >= cend) return;
+    const int t = next_c * 8 + next_k;
+    if (t >= a.n) { next_c = cend; return; }
+    if (lane == 0) {
+      const uint32_t b = issued % kRowBuffers;
+      const uint32_t bytes = (uint32_t)(((a.depth[t] + 3) & ~3) * 4);
+      bulk_row_to_smem(tb0 + b * S, a.dis + a.lab_off[t], bytes, &s_bar[warp][b]);
+    }
+    issued++;
+    if (++next_k == 8) { next_k = 0; next_c += nwarps; }
+  };
+  for (int q = 0; q < kRowBuffers - 1; q++) issue_next();
+
+  for (int c = cbeg + warp; c < cend && !failed; c += nwarps) {
+    const int t0 = c << 3;
+    // deepest ancestor interval of this lane's source holding t0 (binary search)
+    int J = 0;
+    {
+      int h = have ? hs : 1;
+      for (int it = 0; it < nsteps; it++) {
+        if (h - J > 1) {
+          const int mid = (J + h) >> 1;
+          const bool p = (__ldg(lo + mid) <= t0) && (t0 < __ldg(hi + mid));
+          J = p ? mid : J;
+          h = p ? h : mid;
+        }
+      }
+    }
+    int hiJ = have ? __ldg(hi + J) : 0x7fffffff;
+    int loN = (have && J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
+    uint32_t pending = 0;  // targets whose counts are gathered after the chunk
+    const int kend = min(8, a.n - t0);
+    for (int k = 0; k < kend; k++) {
+      const int t = t0 + k;
+      // advance the interval: targets grow, so t leaves intervals on the right and enters a deeper
+      // one only at its first id (one ancestor interval starts at each preorder id)
+      if (have && k > 0) {
+        if (t >= hiJ) {
+          do { J--; hiJ = __ldg(hi + J); } while (t >= hiJ);
+          loN = __ldg(lo + J + 1);
+        } else if (t == loN) {
+          J++;
+          hiJ = __ldg(hi + J);
+          loN = (J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
+        }
+      }
+      issue_next();
+      const uint32_t b = done % kRowBuffers;
+      if (!mbar_wait(&s_bar[warp][b], (done / kRowBuffers) & 1)) {
+        failed = true;
+        break;
+      }
+      done++;
+      const int32_t *tbuf = tb0 + b * S;
+      const int hl = have ? J + 1 : 0;
+      uint32_t m1 = 0xffffffffu, m2 = 0xffffffffu, n1 = 0xffffffffu, n2 = 0xffffffffu;
+      const int full8 = hl & ~7;
+      int j = 0;
+      for (; j < full8; j += 8) {
+        const uint4 x = *reinterpret_cast<const uint4 *>(srow + j);
+        const uint4 y = *reinterpret_cast<const uint4 *>(tbuf + j);
+        const uint4 x2 = *reinterpret_cast<const uint4 *>(srow + j + 4);
+        const uint4 y2 = *reinterpret_cast<const uint4 *>(tbuf + j + 4);
+        const uint32_t v0 = x.x + (y.x << B), v1 = x.y + (y.y << B), v2 = x.z + (y.z << B), v3 = x.w + (y.w << B);
+        const uint32_t u0 = x2.x + (y2.x << B), u1 = x2.y + (y2.y << B), u2 = x2.z + (y2.z << B),
+                       u3 = x2.w + (y2.w << B);
+        m1 = __vimin3_u32(m1, v0, v1);
+        n1 = __vimin3_u32(n1, u0, u1);
+        m1 = __vimin3_u32(m1, v2, v3);
+        n1 = __vimin3_u32(n1, u2, u3);
+        m2 = __vimin3_u32(m2, v0 ^ mask, v1 ^ mask);
+        n2 = __vimin3_u32(n2, u0 ^ mask, u1 ^ mask);
+        m2 = __vimin3_u32(m2, v2 ^ mask, v3 ^ mask);
+        n2 = __vimin3_u32(n2, u2 ^ mask, u3 ^ mask);
+      }
+      for (; j < hl; j += 4) {
+        const uint4 x = *reinterpret_cast<const uint4 *>(srow + j);
+        const uint4 y = *reinterpret_cast<const uint4 *>(tbuf + j);
+        const uint32_t v0 = x.x + (y.x << B);
+        const uint32_t v1 = (j + 1 < hl) ? x.y + (y.y << B) : 0xffffffffu;
+        const uint32_t v2 = (j + 2 < hl) ? x.z + (y.z << B) : 0xffffffffu;
+        const uint32_t v3 = (j + 3 < hl) ? x.w + (y.w << B) : 0xffffffffu;
+        m1 = __vimin3_u32(m1, v0, v1);
+        m1 = __vimin3_u32(m1, v2, v3);
+        m2 = __vimin3_u32(m2, v0 ^ mask, (j + 1 < hl) ? v1 ^ mask : 0xffffffffu);
+        m2 = __vimin3_u32(m2, (j + 2 < hl) ? v2 ^ mask : 0xffffffffu, (j + 3 < hl) ? v3 ^ mask : 0xffffffffu);
+      }
+      m1 = min(m1, n1);
+      m2 = min(m2, n2);
+      const uint32_t dist = m1 >> B;
+      int cnt = 0, hop = 0;
+      if (COUNTS && have) {
+        if ((m1 ^ m2) == mask) {
+          cnt = (int)(m1 & mask);  // the minimising entry; counts resolved after the chunk
+          pending |= 1u << k;
+        } else {
+          const int64_t toff = a.lab_off[t];
+          unsigned cc = 0;
+          int hh = 0;
+          for (int q = 0; q < hl; q++) {
+            if (((srow[q] + ((uint32_t)tbuf[q] << B)) >> B) == dist) {
+              const int2 cs = __ldg(a.ch + soff + q), ct = __ldg(a.ch + toff + q);
+              cc += (unsigned)cs.x * (unsigned)ct.x;
+              hh = max(hh, cs.y + ct.y);
+            }
+          }
+          cnt = (int)cc;
+          hop = hh;
+        }
+      }
+      if (have) {
+        sdc2[k] = make_int2((int)dist, cnt);
+        if (COUNTS) shp1[k] = hop;
+      }
+      __syncwarp();
+    }
+    if (failed) break;
+    if (kend < 8 && have) {
+      for (int k = kend; k < 8; k++) {
+        sdc2[k] = make_int2(0, 0);
+        if (COUNTS) shp1[k] = 0;
+      }
+    }
+    if (COUNTS && have && pending) {
+      int2 cs8[8], ct8[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        if (pending & (1u << k)) {
+          const int jm = sdc2[k].y;
+          cs8[k] = __ldg(a.ch + soff + jm);
+          ct8[k] = __ldg(a.ch + a.lab_off[t0 + k] + jm);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        if (pending & (1u << k)) {
+          sdc2[k].y = (int)((unsigned)cs8[k].x * (unsigned)ct8[k].x);
+          shp1[k] = cs8[k].y + ct8[k].y;
+        }
+      }
+    }
+    if (COUNTS && have) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) mh = max(mh, shp1[k]);
+    }
+    __syncwarp();
+    {  // the warp's 32 slots x 8 targets are one contiguous block: coalesced 512-byte stores
+      int4 *gdc = reinterpret_cast<int4 *>(a.out_dc + blk(first, t0, a.ns));
+      for (int p = lane; p < gcount * 4; p += 32) gdc[p] = sdc[(p >> 2) * 5 + (p & 3)];
+      if (COUNTS) {
+        int4 *ghp = reinterpret_cast<int4 *>(a.out_hop + blk(first, t0, a.ns));
+        for (int p = lane; p < gcount * 2; p += 32) ghp[p] = shp[(p >> 1) * 3 + (p & 1)];
+      }
+    }
+    __syncwarp();
+  }
+  if (failed) {
+    // record, then give the copies still in flight a bounded chance to land before exiting
+    if (lane == 0 && a.err) atomicCAS(a.err, ERR_NONE, ERR_COPY_TIMEOUT);
+    while (done < issued) {
+      mbar_wait(&s_bar[warp][done % kRowBuffers], (done / kRowBuffers) & 1);
+      done++;
+    }
+    return;
+  }
+  if (COUNTS && have && a.maxhop) atomicMax(a.maxhop + first + lane, mh);
+}
+
 // ------------------------------------------------------------------------------- K3 - K5
 struct DepArgs {
+  const int2 *__restrict__ arc_rng;  // per vertex (first arc, end arc)
+  const int2 *__restrict__ arc_hw;   // per arc (head, weight)
   const int32_t *__restrict__ arc_off;
   const int32_t *__restrict__ arc_head;
   const int32_t *__restrict__ arc_w;
@@ -377,7 +670,8 @@ __device__ __forceinline__ int agg_inc(int *ctr, int key, unsigned act) {
 
 // Pull-form dependency of vertex v (MHLQBC.cu:452-466): delta(v) = sum over DAG arcs v->w of
 // sigma_v * (1 + delta_w) / sigma_w, operation order as the reference (:457).
-__device__ __forceinline__ double pull_delta(const DepArgs &a, const int2 *dc, const double *delta, int v) {
+template <class DC>
+__device__ __forceinline__ double pull_delta(const DepArgs &a, const DC &dc, const double *delta, int v) {
   const int2 dv = dc[v];
   const double sv = (double)dv.y;
   double acc = 0.0;
@@ -390,7 +684,8 @@ __device__ __forceinline__ double pull_delta(const DepArgs &a, const int2 *dc, c
   return acc;
 }
 
-__device__ void backprop_levels(const DepArgs &a, const int2 *dc, double *delta, const int32_t *order,
+template <class DC>
+__device__ void backprop_levels(const DepArgs &a, const DC &dc, double *delta, const int32_t *order,
                                 const int *start, int maxL) {
   for (int L = maxL; L >= 1; --L) {
     const int b = start[L], e = start[L + 1];
@@ -412,8 +707,8 @@ __global__ void __launch_bounds__(256) k_dependency(DepArgs a) {
   if (slot >= a.ns) return;
   const int s = a.src[slot];
   const size_t base = (size_t)slot * a.n_pad;
-  const int2 *dc = a.dc + base;
-  const int32_t *hop = a.hop + base;
+  const RowView<const int2> dc{a.dc, slot, a.ns};
+  const RowView<const int32_t> hop{a.hop, slot, a.ns};
   double *delta = a.delta + base;
   int32_t *order = a.order + base;
 
@@ -451,6 +746,133 @@ __global__ void __launch_bounds__(256) k_dependency(DepArgs a) {
   backprop_levels(a, dc, delta, order, cnt, maxL);
 }
 
+// Warp-per-source form of k_dependency for graphs whose per-source DAG is narrow: no CTA-wide
+// barrier per layer (a __syncwarp orders the layer's delta writes), many sources in flight per SM
+// to cover the gathers' DRAM latency, and the largest layer taken from the label kernel.
+// delta of vertex v with its SP-DAG out-arcs gathered four at a time: the (head, weight) pairs of up
+// to four arcs are loaded together, then their heads' (dist, sigma) and delta together, so a vertex
+// costs two rounds of memory latency per four arcs instead of two per arc.  Same FP64 operation
+// order and arc order as pull_delta.
+template <class DC>
+__device__ __forceinline__ double pull_delta4(const DepArgs &a, const DC &dc, const double *delta, int v) {
+  const int2 dv = dc[v];
+  const int2 rng = a.arc_rng[v];
+  const double sv = (double)dv.y;
+  double acc = 0.0;
+  for (int e = rng.x; e < rng.y; e += 4) {
+    int2 hw[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) hw[q] = (e + q < rng.y) ? a.arc_hw[e + q] : make_int2(-1, 0);
+    int2 dw[4];
+    double dl[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      if (hw[q].x >= 0) {
+        dw[q] = dc[hw[q].x];
+        dl[q] = delta[hw[q].x];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (hw[q].x >= 0 && dw[q].x == dv.x + hw[q].y) acc += sv * (1.0 + dl[q]) / (double)dw[q].y;
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(256, 4) k_dependency_warp(DepArgs a, const int32_t *__restrict__ maxhop, int lcap) {
+  extern __shared__ int smw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int slot = blockIdx.x * nwarps + warp;
+  if (slot >= a.ns) return;
+  const int s = a.src[slot];
+  const size_t base = (size_t)slot * a.n_pad;
+  const RowView<const int2> dc{a.dc, slot, a.ns};
+  const RowView<const int32_t> hop{a.hop, slot, a.ns};
+  double *delta = a.delta + base;
+  int32_t *order = a.order + base;
+  const int maxL = maxhop[slot];
+  int *cnt, *cur;
+  if (maxL + 2 <= lcap) {
+    cnt = smw + warp * 2 * lcap;
+    cur = cnt + lcap;
+  } else {
+    cnt = a.lcnt + (size_t)slot * 2 * (a.n_pad + 2);
+    cur = cnt + (a.n_pad + 2);
+  }
+  for (int i = lane; i <= maxL + 1; i += 32) cnt[i] = 0;
+  __syncwarp();
+  // layer histogram: four loads in flight per lane before the aggregated shared atomics
+  for (int v0 = 0; v0 < a.n; v0 += 128) {
+    int hv[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int v = v0 + q * 32 + lane;
+      hv[q] = (v < a.n && v != s) ? hop[v] : -1;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const unsigned act = __ballot_sync(kFull, hv[q] >= 0);
+      if (hv[q] >= 0) agg_inc(cnt, hv[q], act);
+    }
+  }
+  __syncwarp();
+  {  // exclusive scan of cnt[0..maxL] by the warp
+    const int len = maxL + 1;
+    const int per = (len + 31) / 32;
+    const int b = lane * per, e = min(len, b + per);
+    int local = 0;
+    for (int i = b; i < e; i++) local += cnt[i];
+    int x = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, x, o);
+      if (lane >= o) x += y;
+    }
+    int run = x - local;
+    for (int i = b; i < e; i++) {
+      const int c = cnt[i];
+      cnt[i] = run;
+      cur[i] = run;
+      run += c;
+    }
+    const int total = __shfl_sync(kFull, x, 31);
+    if (lane == 0) cnt[len] = total;
+  }
+  __syncwarp();
+  for (int v0 = 0; v0 < a.n; v0 += 128) {
+    int hv[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int v = v0 + q * 32 + lane;
+      hv[q] = (v < a.n && v != s) ? hop[v] : -1;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const unsigned act = __ballot_sync(kFull, hv[q] >= 0);
+      if (hv[q] >= 0) order[agg_inc(cur, hv[q], act)] = v0 + q * 32 + lane;
+    }
+  }
+  __syncwarp();
+  // layers from the deepest up; two vertices per lane per step so their gathers overlap
+  for (int L = maxL; L >= 1; --L) {
+    const int b = cnt[L], e = cnt[L + 1];
+    for (int idx = b + lane; idx < e; idx += 64) {
+      const bool two = idx + 32 < e;
+      const int v1 = order[idx];
+      const int v2 = two ? order[idx + 32] : v1;
+      const double d1 = pull_delta4(a, dc, delta, v1);
+      const double d2 = two ? pull_delta4(a, dc, delta, v2) : 0.0;
+      delta[v1] = d1;
+      atomicAdd(a.bc + v1, 0.5 * d1);
+      if (two) {
+        delta[v2] = d2;
+        atomicAdd(a.bc + v2, 0.5 * d2);
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // QBC: sigma by Kahn waves on the SP-DAG from H2H distances (QBC.cu:335-344, :485-555), then
 // the same backprop.  hop[] holds the in-degree until a vertex is queued, then its wave.
 __global__ void __launch_bounds__(256) k_kahn_dependency(DepArgs a) {
@@ -460,8 +882,8 @@ __global__ void __launch_bounds__(256) k_kahn_dependency(DepArgs a) {
   if (slot >= a.ns) return;
   const int s = a.src[slot];
   const size_t base = (size_t)slot * a.n_pad;
-  int2 *dc = a.dc + base;
-  int32_t *deg = a.hop + base;
+  const RowView<int2> dc{a.dc, slot, a.ns};
+  const RowView<int32_t> deg{a.hop, slot, a.ns};
   double *delta = a.delta + base;
   int32_t *order = a.order + base;
   int *wave = sh_wave;
@@ -561,10 +983,10 @@ __global__ void k_rows_to_vid(const int2 *__restrict__ dc, const int32_t *__rest
   if (slot >= ns) return;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const int v = vid_of[t];
-    const int2 x = dc[(size_t)slot * n_pad + t];
+    const int2 x = dc[blk(slot, t, ns)];
     dist[(size_t)slot * n + v] = x.x;
     if (cnt) cnt[(size_t)slot * n + v] = (uint32_t)x.y;
-    if (hp) hp[(size_t)slot * n + v] = hop[(size_t)slot * n_pad + t];
+    if (hp) hp[(size_t)slot * n + v] = hop[blk(slot, t, ns)];
   }
 }
 
@@ -623,8 +1045,36 @@ static void launch_label_c(const LabelPlan &p, const LabelArgs &a, int groups, c
   }
 }
 
+template <bool C>
+static void launch_label_packed(const Handle &h, const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
+  constexpr int threads = kPackedThreads;
+  const int S = d->hmax_pad;
+  const size_t smem = (size_t)32 * S * 4 + (size_t)(threads / 32) * (kRowBuffers * S * 4 + kStageInt4 * 16);
+  const int groups = (ns + 31) / 32;
+  int split = h.tuning.split;
+  if (split <= 0) {
+    split = std::max(1, (148 * 4 + groups - 1) / groups);
+    split = std::min(split, std::max(1, (d->n_pad / 8) / (threads / 32)));
+  }
+  a.stride = S;
+  a.split = split;
+  auto kern = k_label_scan_packed<C>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(split, groups);
+  kern<<<grid, threads, smem, st>>>(a);
+  CK(cudaGetLastError());
+}
+
+static bool use_packed(const Handle &h, const DeviceState *d, bool plain) {
+  if (plain || d->packed_bits == 0) return false;
+  const int k = h.tuning.lanes_per_source;
+  const size_t smem = (size_t)(32 + kRowBuffers * kPackedWarps) * d->hmax_pad * 4 + (size_t)kPackedWarps * kStageInt4 * 16;
+  return k == 0 && smem + 2048 <= (size_t)d->smem_optin;
+}
+
 static void launch_label(const Handle &h, DeviceState *d, int buf, int32_t ns, bool plain, cudaStream_t st) {
-  LabelPlan p = plan_label(h, d, ns, plain);
+  const bool packed = use_packed(h, d, plain);
+  LabelPlan p = packed ? LabelPlan{1, 32, d->hmax_pad, 512, 1, 0} : plan_label(h, d, ns, plain);
   LabelArgs a{};
   a.dis = d->dis;
   a.ch = d->ch;
@@ -640,14 +1090,25 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, int32_t ns, b
   a.split = p.split;
   a.out_dc = d->dc[buf];
   a.out_hop = d->hop[buf];
+  a.maxhop = d->maxhop[buf];
+  a.aend = d->aend;
+  a.bits = d->packed_bits;
+  a.err = d->err;
   const int groups = (ns + p.G - 1) / p.G;
+  CK(cudaMemsetAsync(d->maxhop[buf], 0, (size_t)ns * 4, st));
   std::pair<cudaEvent_t, cudaEvent_t> ev{};
   if (d->profiling) {
     ev = take_events(d->ev_lab, d->ev_lab_used);
     CK(cudaEventRecord(ev.first, st));
   }
-  if (h.host.kind == IndexKind::MHL) launch_label_c<true>(p, a, groups, st);
-  else launch_label_c<false>(p, a, groups, st);
+  if (packed) {
+    if (h.host.kind == IndexKind::MHL) launch_label_packed<true>(h, d, a, ns, st);
+    else launch_label_packed<false>(h, d, a, ns, st);
+  } else if (h.host.kind == IndexKind::MHL) {
+    launch_label_c<true>(p, a, groups, st);
+  } else {
+    launch_label_c<false>(p, a, groups, st);
+  }
   if (d->profiling) CK(cudaEventRecord(ev.second, st));
   d->label_launches++;
   d->launches++;
@@ -655,6 +1116,8 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, int32_t ns, b
 
 static DepArgs dep_args(DeviceState *d, int buf, int32_t ns) {
   DepArgs a{};
+  a.arc_rng = d->arc_rng;
+  a.arc_hw = d->arc_hw;
   a.arc_off = d->arc_off;
   a.arc_head = d->arc_head;
   a.arc_w = d->arc_w;
@@ -675,13 +1138,21 @@ static DepArgs dep_args(DeviceState *d, int buf, int32_t ns) {
 static void launch_dep(const Handle &h, DeviceState *d, int buf, int32_t ns, cudaStream_t st) {
   DepArgs a = dep_args(d, buf, ns);
   const int threads = std::max(64, std::min(256, (h.tuning.dep_threads / 32) * 32));
+  const bool warp_form = h.host.kind == IndexKind::MHL && h.tuning.dep_form != 2;
   std::pair<cudaEvent_t, cudaEvent_t> ev{};
   if (d->profiling) {
     ev = take_events(d->ev_dp, d->ev_dp_used);
     CK(cudaEventRecord(ev.first, st));
   }
-  if (h.host.kind == IndexKind::MHL) k_dependency<<<ns, threads, 0, st>>>(a);
-  else k_kahn_dependency<<<ns, threads, 0, st>>>(a);
+  if (warp_form) {
+    constexpr int wpb = 8, lcap = 512;
+    const size_t smem = (size_t)wpb * 2 * lcap * 4;
+    k_dependency_warp<<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
+  } else if (h.host.kind == IndexKind::MHL) {
+    k_dependency<<<ns, threads, 0, st>>>(a);
+  } else {
+    k_kahn_dependency<<<ns, threads, 0, st>>>(a);
+  }
   CK(cudaGetLastError());
   if (d->profiling) CK(cudaEventRecord(ev.second, st));
   d->dep_launches++;
@@ -716,11 +1187,27 @@ void device_upload(Handle &h, int device) {
     d->arc_off = dupload(d, ix.arc_off, st);
     d->arc_head = dupload(d, ix.arc_head, st);
     d->arc_w = dupload(d, ix.arc_w, st);
+    {
+      std::vector<int2> rng((size_t)ix.n), hw(ix.arc_head.size());
+      for (int32_t v = 0; v < ix.n; v++) rng[v] = make_int2(ix.arc_off[v], ix.arc_off[v + 1]);
+      for (size_t e = 0; e < hw.size(); e++) hw[e] = make_int2(ix.arc_head[e], ix.arc_w[e]);
+      d->arc_rng = dupload(d, rng, st);
+      d->arc_hw = dupload(d, hw, st);
+      CK(cudaStreamSynchronize(st));  // the staging vectors die here
+    }
     d->vid_of = dupload(d, ix.vid_of, st);
     d->tid_of = dupload(d, ix.tid_of, st);
     d->lab_off = dupload(d, ix.lab_off, st);
     d->dis = dupload(d, ix.dis, st);
     d->anc = dupload(d, ix.anc, st);
+    d->aend = dupload(d, ix.aend, st);
+    {
+      // packed keys (dist << B) | j need every row index below 2^B and 2*max_label + 1 < 2^(32-B)
+      int B = 1;
+      while ((1 << B) < ix.tree_height) B++;
+      const uint64_t room = (uint64_t)1 << (32 - B);
+      d->packed_bits = (B <= 16 && 2ull * (uint64_t)std::max(ix.max_label, 0) + 2 < room) ? B : 0;
+    }
     if (ix.kind == IndexKind::MHL) {
       d->ch = dmalloc<int2>(d, ix.ch.size() / 2);
       CK(cudaMemcpyAsync(d->ch, ix.ch.data(), ix.ch.size() * 4, cudaMemcpyHostToDevice, st));
@@ -744,6 +1231,7 @@ void device_upload(Handle &h, int device) {
       d->order[b] = dmalloc<int32_t>(d, (size_t)chunk * d->n_pad);
       d->lcnt[b] = dmalloc<int32_t>(d, (size_t)chunk * 2 * (d->n_pad + 2));
       d->src[b] = dmalloc<int32_t>(d, (size_t)chunk);
+      d->maxhop[b] = dmalloc<int32_t>(d, (size_t)chunk);
     }
     d->bc_tid = dmalloc<double>(d, ix.n);
     d->bc_vid = dmalloc<double>(d, ix.n);
@@ -761,12 +1249,12 @@ void device_release(Handle &h) {
   if (!d) return;
   cudaSetDevice(d->device);
   cudaDeviceSynchronize();
-  void *ptrs[] = {d->depth, d->send, d->arc_off, d->arc_head, d->arc_w, d->vid_of, d->tid_of, d->lab_off, d->dis,
-                  d->anc, d->ch, d->bc_tid, d->bc_vid, d->err, d->sources};
+  void *ptrs[] = {d->depth, d->send, d->arc_off, d->arc_head, d->arc_w, d->arc_rng, d->arc_hw, d->vid_of, d->tid_of, d->lab_off, d->dis,
+                  d->anc, d->aend, d->ch, d->bc_tid, d->bc_vid, d->err, d->sources};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (int b = 0; b < 2; b++) {
-    void *q[] = {d->dc[b], d->hop[b], d->delta[b], d->order[b], d->lcnt[b], d->src[b]};
+    void *q[] = {d->dc[b], d->hop[b], d->delta[b], d->order[b], d->lcnt[b], d->src[b], d->maxhop[b]};
     for (void *p : q)
       if (p) cudaFree(p);
     if (d->ev_label[b]) cudaEventDestroy(d->ev_label[b]);
@@ -797,6 +1285,7 @@ static void check_err(DeviceState *d) {
     CK(cudaMemset(d->err, 0, 4));
     throw Error(QBC_EDEVICE, e == ERR_DISCONNECTED ? "device: SP-DAG wave pass did not reach every vertex"
                              : e == ERR_BAD_SOURCE ? "device: source id out of range"
+                             : e == ERR_COPY_TIMEOUT ? "device: label-row copy wait ran out"
                                                    : "device: kernel error word " + std::to_string(e));
   }
 }
@@ -822,12 +1311,12 @@ void device_bc_sources(Handle &h, const int32_t *d_sources0, int32_t ns, double 
     CK(cudaGetLastError());
     d->launches++;
     launch_label(h, d, b, cnt, false, d->s_label);
-    CK(cudaEventRecord(d->ev_label[b], d->s_label));
-    CK(cudaStreamWaitEvent(d->s_dep, d->ev_label[b], 0));
-    launch_dep(h, d, b, cnt, d->s_dep);
-    CK(cudaEventRecord(d->ev_dep[b], d->s_dep));
+    // The dependency pass runs right after the scan on the same stream: run concurrently on a
+    // second stream the two kernels thrash each other's caches and both slow down ~2x.
+    launch_dep(h, d, b, cnt, d->s_label);
+    CK(cudaEventRecord(d->ev_dep[b], d->s_label));
   }
-  CK(cudaEventRecord(d->ev_dep[0], d->s_dep));
+  CK(cudaEventRecord(d->ev_dep[0], d->s_label));
   CK(cudaStreamWaitEvent(user, d->ev_dep[0], 0));
   k_tid_to_vid_f64<<<(d->n + 255) / 256, 256, 0, user>>>(d->bc_tid, d->vid_of, d_bc_vid, d->n, 1);
   CK(cudaGetLastError());

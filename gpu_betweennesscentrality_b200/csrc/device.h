@@ -13,7 +13,8 @@ struct Tuning {
   int32_t label_threads = 256;   // threads per CTA of the label kernel
   int32_t split = 0;             // target ranges per source group; 0 = auto
   int32_t chunk = 0;             // sources per scratch buffer; 0 = auto
-  int32_t dep_threads = 256;     // threads per CTA of the dependency kernel
+  int32_t dep_threads = 256;     // threads per CTA of the CTA-per-source dependency kernel
+  int32_t dep_form = 0;          // 0 auto (warp per source for MHL), 1 warp per source, 2 CTA per source
 };
 
 struct DeviceState;  // opaque, defined in device.cu

@@ -390,6 +390,11 @@ void make_tree(const Graph &g, const Elimination &el, Index &ix) {
     }
     row[h - 1] = t;
   }
+  ix.aend.assign((size_t)o, 0);
+  for (int32_t t = 0; t < n; t++) {
+    const int64_t b = ix.lab_off[t];
+    for (int32_t j = 0; j < ix.depth[t]; j++) ix.aend[b + j] = ix.send[ix.anc[b + j]];
+  }
   // arcs in tid space
   ix.arc_off.assign((size_t)n + 1, 0);
   ix.arc_head.resize(g.head.size());
@@ -463,6 +468,9 @@ Index build_mhl(const Graph &g, int nthreads) {
       }
     }
   });
+  ix.max_label = 0;
+  for (int32_t t = 0; t < ix.n; t++)
+    for (int32_t j = 0; j < ix.depth[t]; j++) ix.max_label = std::max(ix.max_label, ix.dis[ix.lab_off[t] + j]);
   return ix;
 }
 
@@ -510,6 +518,9 @@ Index build_h2h(const Graph &g, const std::vector<int32_t> &node_order, int nthr
       }
     }
   });
+  ix.max_label = 0;
+  for (int32_t t = 0; t < ix.n; t++)
+    for (int32_t j = 0; j < ix.depth[t]; j++) ix.max_label = std::max(ix.max_label, ix.dis[ix.lab_off[t] + j]);
   return ix;
 }
 

@@ -50,6 +50,8 @@ struct Index {
   std::vector<int32_t> dis;      // lab_off[n]
   std::vector<int32_t> ch;       // 2*lab_off[n]: (cnt bits, hop) pairs; MHL only
   std::vector<int32_t> anc;      // lab_off[n]: tid of the ancestor each row entry refers to
+  std::vector<int32_t> aend;     // lab_off[n]: subtree end (send) of that ancestor
+  int32_t max_label = 0;         // largest label distance (decides the packed-key scan)
   // arcs in tid space, each tail's arcs in file order
   std::vector<int32_t> arc_off, arc_head, arc_w;
   int64_t depth_sum = 0;

@@ -85,9 +85,12 @@ void qbc_index_free(qbc_index *idx);
 int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int32_t *send, int64_t *lab_off,
                      int32_t *dis, int32_t *ch, int32_t *anc);
 
-/* Tuning of the batched path: params[0]=sources per CTA (1..32, 0=auto), [1]=threads per CTA of
- * the label kernel, [2]=target split per source group (0=auto), [3]=sources per chunk (0=auto),
- * [4]=threads per CTA of the dependency kernel. */
+/* Tuning of the batched path: params[0]=lanes per source K of the label scan (0=auto: the
+ * packed-key kernel when the index allows it, else the smallest K whose rows fit shared memory;
+ * 1..32 forces the general kernel with 32/K sources per CTA), [1]=threads per CTA of the general
+ * label kernel, [2]=target split per source group (0=auto), [3]=sources per chunk (0=auto),
+ * [4]=threads per CTA of the CTA-per-source dependency kernel, [5]=dependency form (0 auto,
+ * 1 one warp per source, 2 one CTA per source). */
 int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams);
 int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams);
 

@@ -46,6 +46,7 @@ def test_rows_bit_exact_all_sources_2k(g2k):
 
 @pytest.mark.parametrize("lanes", [1, 2, 4, 8, 16, 32])
 def test_rows_identical_across_tunings(g2k, lanes):
+    """the packed-key kernel (auto) and every general-kernel lane split give identical rows"""
     n, u, v, w, g, idx, tc, arcs = g2k
     srcs = np.arange(0, n, 13, dtype=np.int32)
     base = idx.rows(srcs)
@@ -73,6 +74,18 @@ def test_plain_path_matches_batched(g2k):
     srcs = np.arange(0, n, 9, dtype=np.int32)
     assert rel_err(idx.bc_plain(srcs), idx.bc_sources(srcs)) <= BC_RTOL
     assert rel_err(idx.bc_sources(srcs), tc.bc(arcs, srcs)) <= BC_RTOL
+
+
+@pytest.mark.parametrize("form", [1, 2])
+def test_dependency_forms_agree(g2k, form):
+    n, u, v, w, g, idx, tc, arcs = g2k
+    srcs = np.arange(0, n, 5, dtype=np.int32)
+    idx.set_tuning(dep_form=form)
+    try:
+        bc = idx.bc_sources(srcs)
+    finally:
+        idx.set_tuning()
+    assert rel_err(bc, tc.bc(arcs, srcs)) <= BC_RTOL
 
 
 def test_bc_repeatable_and_chunked(g2k):
