@@ -220,7 +220,9 @@ def main():
     info = idx.info()
     n = G.nodenum
     ex_vid = idx.export()["vid_of"]  # tid order keeps each CTA's sources close in the tree
-    shard = np.array_split(ex_vid, world)[rank].astype(np.int32)
+    from gpu_betweennesscentrality_b200.shard import all_reduce_bc, max_over_ranks, shard_sources
+
+    shard = shard_sources(ex_vid, world, rank)
     ns = int(shard.shape[0])
 
     stream = torch.cuda.Stream(device=dev)
@@ -255,10 +257,8 @@ def main():
     clk = clocks.stop()
     ms = sum(a.elapsed_time(b) for a, b in ev)
     if world > 1:
-        t_max = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-        ms = float(t_max.item())
-        dist.all_reduce(d_bc)  # the one exchange: sum of the ranks' partial BC vectors
+        ms = max_over_ranks(ms, device=dev)
+        all_reduce_bc(d_bc)  # the one exchange: sum of the ranks' partial BC vectors
         torch.cuda.synchronize()
     value = n * args.steps / (ms / 1e3)
 
@@ -274,9 +274,7 @@ def main():
         h_bc.numpy()[:] = idx.bc_sources(h_src.numpy())
     e2e_s = time.perf_counter() - t
     if world > 1:
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+        e2e_s = max_over_ranks(e2e_s, device=dev)
     e2e_val = n * e2e_steps / e2e_s
 
     # Roofline of the dominant kernel (the label scan).  Algorithmic bytes follow the per-source

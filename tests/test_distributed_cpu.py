@@ -1,0 +1,76 @@
+"""CPU: the multi-rank path's host logic with two gloo ranks.  Each rank computes the partial BC of
+its contiguous source share (with the oracle, standing in for the device sweep), one all-reduce sums
+them, and the result must equal the single-rank BC; timings reduce to the slowest rank."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from conftest import GOLDEN, ROOT
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, out_dir):
+    import sys
+
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import pyoracle as O
+    from gpu_betweennesscentrality_b200 import synth
+    from gpu_betweennesscentrality_b200.shard import all_reduce_bc, max_over_ranks, shard_sources
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    n, u, v, w = synth.read_graph_lines(os.path.join(GOLDEN, "g2k.txt"))
+    tc, arcs = O.TreeCount(n, u, v, w), O.Arcs(n, u, v, w)
+    order = np.arange(n, dtype=np.int32)[::-1].copy()
+    mine = shard_sources(order, world, rank)
+    part = torch.from_numpy(tc.bc(arcs, mine, nthreads=2))
+    all_reduce_bc(part)
+    slowest = max_over_ranks(10.0 + rank)
+    np.save(os.path.join(out_dir, f"bc{rank}.npy"), part.numpy())
+    np.save(os.path.join(out_dir, f"t{rank}.npy"), np.array([slowest, mine.shape[0]]))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_sum_to_the_full_bc(tmp_path):
+    world = 2
+    mp.start_processes(_rank, args=(world, _free_port(), str(tmp_path)), nprocs=world, start_method="spawn")
+    import sys
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    from gpu_betweennesscentrality_b200 import synth
+
+    n, u, v, w = synth.read_graph_lines(os.path.join(GOLDEN, "g2k.txt"))
+    full = O.TreeCount(n, u, v, w).bc(O.Arcs(n, u, v, w))
+    for r in range(world):
+        bc = np.load(tmp_path / f"bc{r}.npy")
+        assert np.max(np.abs(bc - full) / np.maximum(1.0, np.abs(full))) <= 1e-9
+        t = np.load(tmp_path / f"t{r}.npy")
+        assert t[0] == 11.0
+    sizes = [int(np.load(tmp_path / f"t{r}.npy")[1]) for r in range(world)]
+    assert sum(sizes) == n and abs(sizes[0] - sizes[1]) <= 1
+
+
+def test_shard_sources_partition():
+    from gpu_betweennesscentrality_b200.shard import shard_sources
+
+    order = np.arange(1001, dtype=np.int32)
+    parts = [shard_sources(order, 4, r) for r in range(4)]
+    assert np.array_equal(np.concatenate(parts), order)
+    with pytest.raises(ValueError):
+        shard_sources(order, 2, 2)
