@@ -167,6 +167,46 @@ def cpu_baseline(path, seconds=12.0):
                       f"(OpenMP over sources), {dt:.1f} s"}
 
 
+def rq_measurements(idx, n, sweep_value, args):
+    """Batched RQ (64 query sets, sizes log-uniform in 16..16384, one graph-replayed sweep) against
+    the plain per-set calls, and the served loop under Poisson arrivals at three rates (request sizes
+    log-uniform in 1..8192).  Host-timed through the public API with host buffers."""
+    from gpu_betweennesscentrality_b200.serve import poisson_load, request_sets
+
+    sets = request_sets(n, 64, 16, 16384, seed=2)
+    idx.bc_query_batch(sets)  # capture + warm
+    reps = 3
+    t = time.perf_counter()
+    for _ in range(reps):
+        outs = idx.bc_query_batch(sets)
+    t_batch = (time.perf_counter() - t) / reps
+    k_plain = 4  # 64 sequential per-set sweeps would take 64 sweeps; 4 of them are timed
+    t = time.perf_counter()
+    plain_outs = [idx.bc_query(s) for s in sets[:k_plain]]
+    t_plain_set = (time.perf_counter() - t) / k_plain
+    diff = max(float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) for a, b in zip(outs, plain_outs))
+    batched = {"max_rel_diff_vs_plain": diff, "sets": 64, "query_vertices": int(sum(len(s) for s in sets)), "ms": t_batch * 1e3,
+               "sources_per_s": 64 * n / t_batch,
+               "plain_per_set_ms": t_plain_set * 1e3, "plain_sources_per_s": n / t_plain_set,
+               "speedup_vs_64_sequential": 64 * t_plain_set / t_batch,
+               "note": f"plain = one qbc_bc_query call (one full sweep) per set, {k_plain} of 64 timed; "
+                       "batched = one qbc_bc_query_batch call, one graph-replayed sweep for all 64 sets"}
+    # served: slots = 64 concurrent requests; one turn over the sources takes n / sweep rate
+    turn_s = n / sweep_value
+    slots = 64
+    capacity = slots / turn_s
+    served = {"slots": slots, "turn_ms": turn_s * 1e3, "capacity_requests_per_s": capacity, "rates": []}
+    for i, frac in enumerate((0.5, 0.8, 0.95)):
+        rate = frac * capacity
+        count = max(20, int(rate * args.served_seconds))
+        reqs = request_sets(n, count, 1, 8192, seed=100 + i)
+        with idx.serve(max_active=slots) as srv:
+            r = poisson_load(srv, reqs, rate=rate, seed=3 + i)
+        r["rate_fraction_of_capacity"] = frac
+        served["rates"].append({k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()})
+    return {"batched_rq": batched, "served_rq": served}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -177,6 +217,9 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=0, help="sources per scratch buffer (0: sized from free HBM)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default tuning instead of autotuning")
+    ap.add_argument("--no-rq", action="store_true", help="skip the batched and served RQ measurements")
+    ap.add_argument("--served-seconds", type=float, default=8.0, help="arrival window per served rate")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -220,6 +263,12 @@ def main():
     info = idx.info()
     n = G.nodenum
     ex_vid = idx.export()["vid_of"]  # tid order keeps each CTA's sources close in the tree
+    tune = None
+    if not args.no_autotune and not args.chunk:
+        t = time.perf_counter()
+        sample = ex_vid[:: max(1, n // 8192)][:8192]
+        tune = idx.autotune(sample)
+        tune["seconds"] = round(time.perf_counter() - t, 2)
     from gpu_betweennesscentrality_b200.shard import all_reduce_bc, max_over_ranks, shard_sources
 
     shard = shard_sources(ex_vid, world, rank)
@@ -316,6 +365,9 @@ def main():
         plain = {"value": ps.shape[0] / (time.perf_counter() - t), "unit": "sources/s",
                  "sample": f"{ps.shape[0]} sources spread over the tid order, one label launch + one "
                            f"dependency launch each, host-timed with the final synchronisation"}
+    rq = None
+    if rank == 0 and world == 1 and not args.no_rq:
+        rq = rq_measurements(idx, n, value, args)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(path)
@@ -329,7 +381,7 @@ def main():
                                             "label_entries": int(info[7]), "device_bytes": int(info[5]),
                                             "host_build_s": round(t_build, 3), "read_s": round(t_read, 3),
                                             "upload_s": round(t_upload, 3)},
-                                  "tuning": idx.get_tuning()}),
+                                  "tuning": idx.get_tuning(), "autotune": tune}),
                "e2e": {"value": e2e_val, "unit": "sources/s", "h2d_bytes_per_step": int(4 * ns),
                        "d2h_bytes_per_step": int(8 * n), "steps": e2e_steps},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -353,6 +405,9 @@ def main():
             out["cpu_baseline"] = cpu
         if plain is not None:
             out["plain"] = plain
+            out["batched_vs_plain"] = value / plain["value"]
+        if rq is not None:
+            out.update(rq)
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.barrier(device_ids=[local])

@@ -15,6 +15,7 @@ pointers) used by tests and the benchmark.
 from __future__ import annotations
 
 import ctypes as C
+import json
 from typing import Optional, Sequence
 
 import numpy as np
@@ -123,16 +124,43 @@ class Index:
         check(lib().qbc_index_scan_entries(self.h, ptr(s, i32p), int(s.shape[0]), C.byref(e)))
         return int(e.value)
 
-    TUNING_KEYS = ("lanes_per_source", "label_threads", "split", "chunk", "dep_threads", "dep_form")
+    TUNING_KEYS = ("lanes_per_source", "label_threads", "split", "chunk", "dep_threads", "dep_form", "queue_depth")
 
-    def set_tuning(self, lanes_per_source=0, label_threads=256, split=0, chunk=0, dep_threads=256, dep_form=0):
-        p = i32([lanes_per_source, label_threads, split, chunk, dep_threads, dep_form])
-        check(lib().qbc_index_set_tuning(self.h, ptr(p, i32p), 6))
+    def set_tuning(self, lanes_per_source=0, label_threads=256, split=0, chunk=0, dep_threads=256, dep_form=0,
+                   queue_depth=0):
+        p = i32([lanes_per_source, label_threads, split, chunk, dep_threads, dep_form, queue_depth])
+        check(lib().qbc_index_set_tuning(self.h, ptr(p, i32p), 7))
 
     def get_tuning(self):
-        p = np.zeros(6, np.int32)
-        check(lib().qbc_index_get_tuning(self.h, ptr(p, i32p), 6))
+        p = np.zeros(7, np.int32)
+        check(lib().qbc_index_get_tuning(self.h, ptr(p, i32p), 7))
         return dict(zip(self.TUNING_KEYS, p.tolist()))
+
+    def autotune(self, sample, path: Optional[str] = None) -> dict:
+        """Times candidate tunings on a sweep over ``sample`` (vids), keeps the fastest on the index
+        and returns it; with ``path`` it is also written there as JSON (``load_tuning`` reads it)."""
+        s = i32(sample)
+        p = np.zeros(7, np.int32)
+        ms = C.c_double()
+        check(lib().qbc_autotune(self.h, ptr(s, i32p), int(s.shape[0]), ptr(p, i32p), 7, C.byref(ms)))
+        res = dict(tuning=dict(zip(self.TUNING_KEYS, p.tolist())), ms_per_source=float(ms.value),
+                   sample_sources=int(s.shape[0]), n=self.n)
+        if path:
+            with open(path, "w") as f:
+                json.dump(res, f, indent=1)
+        return res
+
+    def load_tuning(self, path: str) -> dict:
+        with open(path) as f:
+            t = json.load(f)["tuning"]
+        self.set_tuning(**{k: int(t[k]) for k in self.TUNING_KEYS if k in t})
+        return self.get_tuning()
+
+    def serve(self, sources=None, max_active: int = 64, pool_bytes: int = 0, max_queue: int = 0):
+        """Opens the served RQ loop on this index (see ``serve.Server``)."""
+        from .serve import Server
+
+        return Server(self, sources, max_active, pool_bytes, max_queue)
 
     def profile(self, on: bool = True) -> None:
         check(lib().qbc_index_profile(self.h, 1 if on else 0))

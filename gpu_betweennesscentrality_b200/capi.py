@@ -54,6 +54,13 @@ SIGNATURES = {
     "qbc_index_stats": (C.c_int, [vp, f64p]),
     "qbc_bc_source_static": (C.c_int, [vp, C.c_int32, vp, vp]),
     "qbc_rows": (C.c_int, [vp, i32p, C.c_int32, i32p, u32p, i32p]),
+    "qbc_autotune": (C.c_int, [vp, i32p, C.c_int32, i32p, C.c_int32, f64p]),
+    "qbc_serve_open": (C.c_int, [vp, i32p, C.c_int32, i64p, C.c_int32, C.POINTER(vp)]),
+    "qbc_serve_submit": (C.c_int, [vp, i32p, C.c_int32, i64p]),
+    "qbc_serve_poll": (C.c_int, [vp, C.c_int64, f64p, f64p, i32p]),
+    "qbc_serve_wait": (C.c_int, [vp, C.c_int64, C.c_double, f64p, f64p, i32p]),
+    "qbc_serve_stats": (C.c_int, [vp, f64p, C.c_int32]),
+    "qbc_serve_close": (C.c_int, [vp]),
 }
 
 

@@ -13,7 +13,13 @@ struct qbc_graph {
 };
 struct qbc_index {
   qbc::Handle h;
-  ~qbc_index() { qbc::device_release(h); }
+  ~qbc_index() {
+    if (h.server) qbc::serve_close(h.server);
+    qbc::device_release(h);
+  }
+};
+struct qbc_server {
+  qbc::Server *s;
 };
 
 namespace {
@@ -39,6 +45,10 @@ int guarded(F &&f) {
 
 void need(bool ok, const char *what) {
   if (!ok) throw qbc::Error(QBC_EINVAL, what);
+}
+
+void not_serving(const qbc_index *idx) {
+  if (idx->h.server) throw qbc::Error(QBC_EBUSY, "the index is serving requests: close its server first");
 }
 }  // namespace
 
@@ -132,6 +142,7 @@ int qbc_index_build(const qbc_graph *g, int kind, const int32_t *node_order, int
 int qbc_index_upload(qbc_index *idx, int device) {
   return guarded([&] {
     need(idx, "null index");
+    not_serving(idx);
     qbc::device_upload(idx->h, device);
   });
 }
@@ -139,6 +150,7 @@ int qbc_index_upload(qbc_index *idx, int device) {
 int qbc_index_release_device(qbc_index *idx) {
   return guarded([&] {
     need(idx, "null index");
+    not_serving(idx);
     qbc::device_release(idx->h);
   });
 }
@@ -191,15 +203,17 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
   return guarded([&] {
     need(idx && (nparams == 0 || params), "null argument");
     qbc::Tuning &t = idx->h.tuning;
-    int32_t *f[] = {&t.lanes_per_source, &t.label_threads, &t.split, &t.chunk, &t.dep_threads, &t.dep_form};
+    not_serving(idx);
+    int32_t *f[] = {&t.lanes_per_source, &t.label_threads, &t.split, &t.chunk, &t.dep_threads, &t.dep_form, &t.queue_depth};
     if (nparams > 0) {
       int32_t k = params[0];
       need(k == 0 || k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32, "lanes per source must be 0 or a power of two <= 32");
     }
     const int32_t old_chunk = t.chunk;
     if (nparams > 5) need(params[5] >= 0 && params[5] <= 2, "dependency form must be 0, 1 or 2");
-    for (int32_t i = 0; i < nparams && i < 6; i++) *f[i] = params[i];
-    if (nparams > 3 && t.chunk != old_chunk && idx->h.dev) qbc::device_upload(idx->h, qbc::device_id(idx->h));
+    if (nparams > 6) need(params[6] == 0 || (params[6] >= 64 && params[6] <= 2048), "queue depth must be 0 or in [64, 2048]");
+    for (int32_t i = 0; i < nparams && i < 7; i++) *f[i] = params[i];
+    if (nparams > 3 && t.chunk != old_chunk && idx->h.dev) qbc::device_set_chunk(idx->h, t.chunk);
   });
 }
 
@@ -207,17 +221,15 @@ int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams)
   return guarded([&] {
     need(idx && (nparams == 0 || params), "null argument");
     const qbc::Tuning &t = idx->h.tuning;
-    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form};
-    for (int32_t i = 0; i < nparams && i < 6; i++) params[i] = f[i];
+    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth};
+    for (int32_t i = 0; i < nparams && i < 7; i++) params[i] = f[i];
   });
 }
 
 int qbc_bc_all(qbc_index *idx, double *bc_out) {
   return guarded([&] {
     need(idx && bc_out, "null argument");
-    std::vector<int32_t> all((size_t)idx->h.host.n);
-    for (int32_t t = 0; t < idx->h.host.n; t++) all[t] = idx->h.host.vid_of[t];  // tid order
-    qbc::host_bc_sources(idx->h, all.data(), (int32_t)all.size(), bc_out);
+    qbc::host_bc_sweep(idx->h, nullptr, 0, bc_out);
   });
 }
 
@@ -245,14 +257,7 @@ int qbc_bc_sources_device(qbc_index *idx, const int32_t *d_sources0, int32_t ns,
 int qbc_bc_query(qbc_index *idx, const int32_t *points0, int32_t q, double *out) {
   return guarded([&] {
     need(idx && q >= 0 && (q == 0 || (points0 && out)), "null argument");
-    const int32_t n = idx->h.host.n;
-    for (int32_t i = 0; i < q; i++)
-      if (points0[i] < 0 || points0[i] >= n) throw qbc::Error(QBC_EINVAL, "query id out of range");
-    std::vector<double> bc((size_t)n);
-    std::vector<int32_t> all((size_t)n);
-    for (int32_t t = 0; t < n; t++) all[t] = idx->h.host.vid_of[t];
-    qbc::host_bc_sources(idx->h, all.data(), n, bc.data());
-    for (int32_t i = 0; i < q; i++) out[i] = bc[points0[i]];
+    qbc::host_query_batch(idx->h, points0, q, nullptr, 0, out);
   });
 }
 
@@ -260,20 +265,12 @@ int qbc_bc_query_batch(qbc_index *idx, const int32_t *points0, const int32_t *se
                        const int32_t *sources0, int32_t ns, double *out) {
   return guarded([&] {
     need(idx && set_off && nsets >= 0, "null argument");
-    const int32_t n = idx->h.host.n;
+    need(set_off[0] == 0, "set offsets must start at 0");
+    for (int32_t k = 0; k < nsets; k++) need(set_off[k + 1] >= set_off[k], "set offsets must not decrease");
     const int32_t total = nsets ? set_off[nsets] : 0;
     need(total == 0 || (points0 && out), "null argument");
-    for (int32_t i = 0; i < total; i++)
-      if (points0[i] < 0 || points0[i] >= n) throw qbc::Error(QBC_EINVAL, "query id out of range");
-    std::vector<double> bc((size_t)n);
-    if (sources0) {
-      qbc::host_bc_sources(idx->h, sources0, ns, bc.data());
-    } else {
-      std::vector<int32_t> all((size_t)n);
-      for (int32_t t = 0; t < n; t++) all[t] = idx->h.host.vid_of[t];
-      qbc::host_bc_sources(idx->h, all.data(), n, bc.data());
-    }
-    for (int32_t i = 0; i < total; i++) out[i] = bc[points0[i]];
+    need(!sources0 || ns > 0, "empty source list");
+    qbc::host_query_batch(idx->h, points0, total, sources0, ns, out);
   });
 }
 
@@ -302,6 +299,65 @@ int qbc_rows(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *dist,
   return guarded([&] {
     need(idx && dist && ns >= 0 && (ns == 0 || sources0), "null argument");
     qbc::host_rows(idx->h, sources0, ns, dist, cnt, hop);
+  });
+}
+
+int qbc_autotune(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *params, int32_t nparams,
+                 double *ms_per_source) {
+  return guarded([&] {
+    need(idx && sources0 && ns > 0, "null argument");
+    double ms = 0.0;
+    qbc::autotune(idx->h, sources0, ns, &ms);
+    if (ms_per_source) *ms_per_source = ms;
+    const qbc::Tuning &t = idx->h.tuning;
+    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth};
+    for (int32_t i = 0; params && i < nparams && i < 7; i++) params[i] = f[i];
+  });
+}
+
+int qbc_serve_open(qbc_index *idx, const int32_t *sources0, int32_t ns, const int64_t *opts, int32_t nopts,
+                   qbc_server **out) {
+  return guarded([&] {
+    need(idx && out && (nopts == 0 || opts) && (!sources0 || ns > 0), "null argument");
+    auto p = std::make_unique<qbc_server>();
+    p->s = qbc::serve_open(idx->h, sources0, ns, opts, nopts);
+    *out = p.release();
+  });
+}
+
+int qbc_serve_submit(qbc_server *srv, const int32_t *points0, int32_t q, int64_t *ticket) {
+  return guarded([&] {
+    need(srv && ticket, "null argument");
+    *ticket = qbc::serve_submit(srv->s, points0, q);
+  });
+}
+
+int qbc_serve_poll(qbc_server *srv, int64_t ticket, double *out, double *times, int32_t *done) {
+  return guarded([&] {
+    need(srv && done, "null argument");
+    *done = qbc::serve_poll(srv->s, ticket, out, times);
+  });
+}
+
+int qbc_serve_wait(qbc_server *srv, int64_t ticket, double timeout_s, double *out, double *times, int32_t *done) {
+  return guarded([&] {
+    need(srv && done, "null argument");
+    *done = qbc::serve_wait(srv->s, ticket, timeout_s, out, times);
+  });
+}
+
+int qbc_serve_stats(qbc_server *srv, double *out, int32_t nout) {
+  return guarded([&] {
+    need(srv && (nout == 0 || out), "null argument");
+    qbc::serve_stats(srv->s, out, nout);
+  });
+}
+
+int qbc_serve_close(qbc_server *srv) {
+  return guarded([&] {
+    if (!srv) return;
+    qbc::serve_close(srv->s);
+    delete srv;
   });
 }
 

@@ -31,20 +31,9 @@
 #include <string>
 #include <vector>
 
-#include "../../include/qbc_b200.h"
-#include "device.h"
+#include "device_state.h"
 
 namespace qbc {
-
-#define CK(call)                                                                                    \
-  do {                                                                                              \
-    cudaError_t e_ = (call);                                                                        \
-    if (e_ != cudaSuccess)                                                                          \
-      throw Error(e_ == cudaErrorMemoryAllocation ? QBC_ENOMEM : QBC_ECUDA,                         \
-                  std::string(#call) + ": " + cudaGetErrorString(e_));                              \
-  } while (0)
-
-enum : int32_t { ERR_NONE = 0, ERR_HOP_CAP = 1, ERR_DISCONNECTED = 2, ERR_BAD_SOURCE = 3, ERR_COPY_TIMEOUT = 4 };
 
 constexpr int kLayerCap = 4094;  // shared-memory layer counters; deeper DAGs use global memory
 constexpr unsigned kFull = 0xffffffffu;
@@ -63,69 +52,6 @@ struct RowView {
   int slot, ns;
   __device__ __forceinline__ T &operator[](int t) const { return p[blk(slot, t, ns)]; }
 };
-
-// ------------------------------------------------------------------------------- state
-struct DeviceState {
-  int device = 0;
-  cudaStream_t s_label = nullptr, s_dep = nullptr;
-  cudaEvent_t ev_label[2] = {nullptr, nullptr}, ev_dep[2] = {nullptr, nullptr}, ev_start = nullptr;
-  int32_t n = 0, n_pad = 0, hmax_pad = 0;
-  int32_t *depth = nullptr, *send = nullptr, *arc_off = nullptr, *arc_head = nullptr, *arc_w = nullptr;
-  int2 *arc_rng = nullptr, *arc_hw = nullptr;
-  int32_t *vid_of = nullptr, *tid_of = nullptr, *dis = nullptr, *anc = nullptr, *aend = nullptr;
-  int32_t packed_bits = 0;  // > 0: the packed-key label scan applies
-  int64_t *lab_off = nullptr;
-  int2 *ch = nullptr;
-  // scratch, two buffers of `chunk` slots
-  int32_t chunk = 0;
-  int2 *dc[2] = {nullptr, nullptr};
-  int32_t *hop[2] = {nullptr, nullptr};
-  double *delta[2] = {nullptr, nullptr};
-  int32_t *order[2] = {nullptr, nullptr};
-  int32_t *lcnt[2] = {nullptr, nullptr};
-  int32_t *src[2] = {nullptr, nullptr};
-  int32_t *maxhop[2] = {nullptr, nullptr};
-  double *bc_tid = nullptr;
-  double *bc_vid = nullptr;
-  int32_t *sources = nullptr;  // staging for host source lists
-  int32_t sources_cap = 0;
-  int32_t *err = nullptr;
-  int64_t bytes = 0;
-  int smem_optin = 0;
-  // optional per-launch timing of the two main kernels (events on their launching streams)
-  bool profiling = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_lab, ev_dp;
-  size_t ev_lab_used = 0, ev_dp_used = 0;
-  double label_ms = 0.0, dep_ms = 0.0;
-  int64_t label_launches = 0, dep_launches = 0, launches = 0;
-};
-
-static std::pair<cudaEvent_t, cudaEvent_t> take_events(std::vector<std::pair<cudaEvent_t, cudaEvent_t>> &pool,
-                                                       size_t &used) {
-  if (used == pool.size()) {
-    cudaEvent_t a, b;
-    CK(cudaEventCreate(&a));
-    CK(cudaEventCreate(&b));
-    pool.push_back({a, b});
-  }
-  return pool[used++];
-}
-
-template <class T>
-static T *dmalloc(DeviceState *d, size_t count) {
-  void *p = nullptr;
-  if (count == 0) count = 1;
-  CK(cudaMalloc(&p, count * sizeof(T)));
-  d->bytes += (int64_t)(count * sizeof(T));
-  return (T *)p;
-}
-
-template <class T>
-static T *dupload(DeviceState *d, const std::vector<T> &v, cudaStream_t s) {
-  T *p = dmalloc<T>(d, v.size());
-  if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
-  return p;
-}
 
 // ------------------------------------------------------------------------------- K1 + K2
 struct LabelArgs {
@@ -1072,7 +998,8 @@ static bool use_packed(const Handle &h, const DeviceState *d, bool plain) {
   return k == 0 && smem + 2048 <= (size_t)d->smem_optin;
 }
 
-static void launch_label(const Handle &h, DeviceState *d, int buf, int32_t ns, bool plain, cudaStream_t st) {
+static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t *src, int32_t ns, bool plain,
+                         cudaStream_t st) {
   const bool packed = use_packed(h, d, plain);
   LabelPlan p = packed ? LabelPlan{1, 32, d->hmax_pad, 512, 1, 0} : plan_label(h, d, ns, plain);
   LabelArgs a{};
@@ -1082,7 +1009,7 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, int32_t ns, b
   a.lab_off = d->lab_off;
   a.depth = d->depth;
   a.send = d->send;
-  a.src = d->src[buf];
+  a.src = src;
   a.ns = ns;
   a.n = d->n;
   a.n_pad = d->n_pad;
@@ -1114,14 +1041,14 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, int32_t ns, b
   d->launches++;
 }
 
-static DepArgs dep_args(DeviceState *d, int buf, int32_t ns) {
+static DepArgs dep_args(DeviceState *d, int buf, const int32_t *src, int32_t ns) {
   DepArgs a{};
   a.arc_rng = d->arc_rng;
   a.arc_hw = d->arc_hw;
   a.arc_off = d->arc_off;
   a.arc_head = d->arc_head;
   a.arc_w = d->arc_w;
-  a.src = d->src[buf];
+  a.src = src;
   a.ns = ns;
   a.n = d->n;
   a.n_pad = d->n_pad;
@@ -1135,8 +1062,8 @@ static DepArgs dep_args(DeviceState *d, int buf, int32_t ns) {
   return a;
 }
 
-static void launch_dep(const Handle &h, DeviceState *d, int buf, int32_t ns, cudaStream_t st) {
-  DepArgs a = dep_args(d, buf, ns);
+static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *src, int32_t ns, cudaStream_t st) {
+  DepArgs a = dep_args(d, buf, src, ns);
   const int threads = std::max(64, std::min(256, (h.tuning.dep_threads / 32) * 32));
   const bool warp_form = h.host.kind == IndexKind::MHL && h.tuning.dep_form != 2;
   std::pair<cudaEvent_t, cudaEvent_t> ev{};
@@ -1145,8 +1072,11 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, int32_t ns, cud
     CK(cudaEventRecord(ev.first, st));
   }
   if (warp_form) {
-    constexpr int wpb = 8, lcap = 512;
+    constexpr int wpb = 8;
+    const int lcap = h.tuning.queue_depth > 0 ? std::min(2048, std::max(64, h.tuning.queue_depth)) : 512;
     const size_t smem = (size_t)wpb * 2 * lcap * 4;
+    if (smem > 48 * 1024)
+      CK(cudaFuncSetAttribute(k_dependency_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_dependency_warp<<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
   } else if (h.host.kind == IndexKind::MHL) {
     k_dependency<<<ns, threads, 0, st>>>(a);
@@ -1157,6 +1087,75 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, int32_t ns, cud
   if (d->profiling) CK(cudaEventRecord(ev.second, st));
   d->dep_launches++;
   d->launches++;
+}
+
+void launch_chunk(const Handle &h, DeviceState *d, const int32_t *d_src_tid, int32_t cnt, int buf, cudaStream_t st) {
+  launch_label(h, d, buf, d_src_tid, cnt, false, st);
+  launch_dep(h, d, buf, d_src_tid, cnt, st);
+}
+
+void launch_tid_to_vid(DeviceState *d, const double *in_tid, double *out_vid, int accumulate, cudaStream_t st) {
+  k_tid_to_vid_f64<<<(d->n + 255) / 256, 256, 0, st>>>(in_tid, d->vid_of, out_vid, d->n, accumulate);
+  CK(cudaGetLastError());
+  d->launches++;
+}
+
+void launch_vid_to_tid(DeviceState *d, const int32_t *vids, int32_t *tids, int32_t cnt, cudaStream_t st) {
+  if (cnt <= 0) return;
+  k_vid_to_tid<<<(cnt + 255) / 256, 256, 0, st>>>(vids, d->tid_of, tids, cnt, d->n, d->err);
+  CK(cudaGetLastError());
+  d->launches++;
+}
+
+// Per-source scratch: two buffers of `chunk` source slots (24 B per vertex and slot plus the layer
+// counters).  `chunk` comes from the tuning, else from the free memory left after the index.
+static void free_scratch(DeviceState *d) {
+  sweep_cache_free(d);
+  for (int b = 0; b < 2; b++) {
+    void *q[] = {d->dc[b], d->hop[b], d->delta[b], d->order[b], d->lcnt[b], d->src[b], d->maxhop[b]};
+    for (void *p : q)
+      if (p) cudaFree(p);
+    d->dc[b] = nullptr;
+    d->hop[b] = d->order[b] = d->lcnt[b] = d->src[b] = d->maxhop[b] = nullptr;
+    d->delta[b] = nullptr;
+  }
+  d->bytes -= d->scratch_bytes;
+  d->scratch_bytes = 0;
+  d->chunk = 0;
+}
+
+static void alloc_scratch(Handle &h, DeviceState *d) {
+  const Index &ix = h.host;
+  const int64_t before = d->bytes;
+  const size_t per_slot = (size_t)d->n_pad * (8 + 4 + 8 + 4) + (size_t)2 * (d->n_pad + 2) * 4 + 4;
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  int32_t chunk = h.tuning.chunk;
+  if (chunk <= 0) {
+    const size_t budget = std::min<size_t>(free_b / 4, (size_t)24 << 30);
+    chunk = (int32_t)std::max<size_t>(32, std::min<size_t>(4096, budget / (2 * per_slot)));
+    chunk = std::max(32, (chunk / 32) * 32);
+  }
+  chunk = std::min<int32_t>(chunk, std::max(32, (ix.n + 31) / 32 * 32));
+  d->chunk = chunk;
+  for (int b = 0; b < 2; b++) {
+    d->dc[b] = dmalloc<int2>(d, (size_t)chunk * d->n_pad);
+    d->hop[b] = dmalloc<int32_t>(d, (size_t)chunk * d->n_pad);
+    d->delta[b] = dmalloc<double>(d, (size_t)chunk * d->n_pad);
+    d->order[b] = dmalloc<int32_t>(d, (size_t)chunk * d->n_pad);
+    d->lcnt[b] = dmalloc<int32_t>(d, (size_t)chunk * 2 * (d->n_pad + 2));
+    d->src[b] = dmalloc<int32_t>(d, (size_t)chunk);
+    d->maxhop[b] = dmalloc<int32_t>(d, (size_t)chunk);
+  }
+  d->scratch_bytes = d->bytes - before;
+}
+
+void device_set_chunk(Handle &h, int32_t chunk) {
+  DeviceState *d = need_dev(h);
+  CK(cudaDeviceSynchronize());
+  free_scratch(d);
+  h.tuning.chunk = chunk;
+  alloc_scratch(h, d);
 }
 
 // ------------------------------------------------------------------------------- upload
@@ -1212,27 +1211,7 @@ void device_upload(Handle &h, int device) {
       d->ch = dmalloc<int2>(d, ix.ch.size() / 2);
       CK(cudaMemcpyAsync(d->ch, ix.ch.data(), ix.ch.size() * 4, cudaMemcpyHostToDevice, st));
     }
-    // scratch: two buffers of `chunk` source slots
-    const size_t per_slot = (size_t)d->n_pad * (8 + 4 + 8 + 4) + (size_t)2 * (d->n_pad + 2) * 4 + 4;
-    size_t free_b = 0, total_b = 0;
-    CK(cudaMemGetInfo(&free_b, &total_b));
-    int32_t chunk = h.tuning.chunk;
-    if (chunk <= 0) {
-      const size_t budget = std::min<size_t>(free_b / 4, (size_t)24 << 30);
-      chunk = (int32_t)std::max<size_t>(32, std::min<size_t>(4096, budget / (2 * per_slot)));
-      chunk = std::max(32, (chunk / 32) * 32);
-    }
-    chunk = std::min<int32_t>(chunk, std::max(32, (ix.n + 31) / 32 * 32));
-    d->chunk = chunk;
-    for (int b = 0; b < 2; b++) {
-      d->dc[b] = dmalloc<int2>(d, (size_t)chunk * d->n_pad);
-      d->hop[b] = dmalloc<int32_t>(d, (size_t)chunk * d->n_pad);
-      d->delta[b] = dmalloc<double>(d, (size_t)chunk * d->n_pad);
-      d->order[b] = dmalloc<int32_t>(d, (size_t)chunk * d->n_pad);
-      d->lcnt[b] = dmalloc<int32_t>(d, (size_t)chunk * 2 * (d->n_pad + 2));
-      d->src[b] = dmalloc<int32_t>(d, (size_t)chunk);
-      d->maxhop[b] = dmalloc<int32_t>(d, (size_t)chunk);
-    }
+    alloc_scratch(h, d);
     d->bc_tid = dmalloc<double>(d, ix.n);
     d->bc_vid = dmalloc<double>(d, ix.n);
     d->err = dmalloc<int32_t>(d, 1);
@@ -1253,10 +1232,8 @@ void device_release(Handle &h) {
                   d->anc, d->aend, d->ch, d->bc_tid, d->bc_vid, d->err, d->sources};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  free_scratch(d);
   for (int b = 0; b < 2; b++) {
-    void *q[] = {d->dc[b], d->hop[b], d->delta[b], d->order[b], d->lcnt[b], d->src[b], d->maxhop[b]};
-    for (void *p : q)
-      if (p) cudaFree(p);
     if (d->ev_label[b]) cudaEventDestroy(d->ev_label[b]);
     if (d->ev_dep[b]) cudaEventDestroy(d->ev_dep[b]);
   }
@@ -1272,13 +1249,14 @@ void device_release(Handle &h) {
 int64_t device_bytes(const Handle &h) { return h.dev ? h.dev->bytes : 0; }
 int device_id(const Handle &h) { return h.dev ? h.dev->device : -1; }
 
-static DeviceState *need_dev(Handle &h) {
+DeviceState *need_dev(Handle &h) {
   if (!h.dev) throw Error(QBC_EINVAL, "index is not on a device: call qbc_index_upload first");
+  if (h.server) throw Error(QBC_EBUSY, "the index is serving requests: close its server first");
   CK(cudaSetDevice(h.dev->device));
   return h.dev;
 }
 
-static void check_err(DeviceState *d) {
+void check_err(DeviceState *d) {
   int32_t e = 0;
   CK(cudaMemcpy(&e, d->err, 4, cudaMemcpyDeviceToHost));
   if (e != ERR_NONE) {
@@ -1310,10 +1288,10 @@ void device_bc_sources(Handle &h, const int32_t *d_sources0, int32_t ns, double 
     k_vid_to_tid<<<(cnt + 255) / 256, 256, 0, d->s_label>>>(d_sources0 + off, d->tid_of, d->src[b], cnt, d->n, d->err);
     CK(cudaGetLastError());
     d->launches++;
-    launch_label(h, d, b, cnt, false, d->s_label);
+    launch_label(h, d, b, d->src[b], cnt, false, d->s_label);
     // The dependency pass runs right after the scan on the same stream: run concurrently on a
     // second stream the two kernels thrash each other's caches and both slow down ~2x.
-    launch_dep(h, d, b, cnt, d->s_label);
+    launch_dep(h, d, b, d->src[b], cnt, d->s_label);
     CK(cudaEventRecord(d->ev_dep[b], d->s_label));
   }
   CK(cudaEventRecord(d->ev_dep[0], d->s_label));
@@ -1393,8 +1371,8 @@ void host_bc_plain(Handle &h, const int32_t *sources0, int32_t ns, double *bc_ou
   for (int32_t i = 0; i < ns; i++) {
     k_vid_to_tid<<<1, 32, 0, st>>>(ds + i, d->tid_of, d->src[0], 1, d->n, d->err);
     CK(cudaGetLastError());
-    launch_label(h, d, 0, 1, true, st);
-    launch_dep(h, d, 0, 1, st);
+    launch_label(h, d, 0, d->src[0], 1, true, st);
+    launch_dep(h, d, 0, d->src[0], 1, st);
   }
   k_tid_to_vid_f64<<<(d->n + 255) / 256, 256, 0, st>>>(d->bc_tid, d->vid_of, d->bc_vid, d->n, 0);
   CK(cudaGetLastError());
@@ -1419,11 +1397,11 @@ void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, ui
       const int32_t c = std::min(step, ns - off);
       k_vid_to_tid<<<(c + 255) / 256, 256, 0, st>>>(ds + off, d->tid_of, d->src[0], c, n, d->err);
       CK(cudaGetLastError());
-      launch_label(h, d, 0, c, false, st);
+      launch_label(h, d, 0, d->src[0], c, false, st);
       if (h.host.kind == IndexKind::H2H && (cnt || hop)) {
         // sigma and waves by the Kahn pass; BC accumulation goes to a scratch target
         CK(cudaMemsetAsync(d->bc_tid, 0, (size_t)n * 8, st));
-        launch_dep(h, d, 0, c, st);
+        launch_dep(h, d, 0, d->src[0], c, st);
       }
       dim3 grid((n + 255) / 256, c);
       k_rows_to_vid<<<grid, 256, 0, st>>>(d->dc[0], d->hop[0], d->vid_of, n, d->n_pad, c, o_d, o_c, o_h);

@@ -15,18 +15,23 @@ struct Tuning {
   int32_t chunk = 0;             // sources per scratch buffer; 0 = auto
   int32_t dep_threads = 256;     // threads per CTA of the CTA-per-source dependency kernel
   int32_t dep_form = 0;          // 0 auto (warp per source for MHL), 1 warp per source, 2 CTA per source
+  int32_t queue_depth = 0;       // level-queue layers held in shared memory by the warp form; 0 = 512
 };
 
-struct DeviceState;  // opaque, defined in device.cu
+struct DeviceState;  // opaque, defined in device_state.h
+struct Server;       // served request loop, defined in sweep.cu
 
 struct Handle {
   Index host;
   Tuning tuning;
   DeviceState *dev = nullptr;
+  Server *server = nullptr;  // while set, the index's device state belongs to that server
 };
 
 void device_upload(Handle &h, int device);
 void device_release(Handle &h);
+// Reallocates the per-source scratch for `chunk` source slots (0 = sized from free memory).
+void device_set_chunk(Handle &h, int32_t chunk);
 int64_t device_bytes(const Handle &h);
 int device_id(const Handle &h);  // -1 when not uploaded
 
@@ -44,6 +49,21 @@ void device_profiling(Handle &h, bool on);
 void device_stats(Handle &h, double *out);
 // rows of each listed source in vid order (cnt/hop may be null)
 void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, uint32_t *cnt, int32_t *hop);
+
+// Batched sweeps (sweep.cu): the sweep over a source list (nullptr = all vertices) is captured once
+// into a CUDA graph per source list and tuning, and replayed.
+void host_bc_sweep(Handle &h, const int32_t *sources0, int32_t ns, double *bc_out);
+// BC of `total` query vertices (the concatenated sets of a batch) from one sweep.
+void host_query_batch(Handle &h, const int32_t *points0, int64_t total, const int32_t *sources0, int32_t ns, double *out);
+// Times candidate tunings on a sweep over the listed sources and keeps the fastest.
+void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_source);
+// Served request loop (see sweep.cu).
+Server *serve_open(Handle &h, const int32_t *sources0, int32_t ns, const int64_t *opts, int32_t nopts);
+int64_t serve_submit(Server *s, const int32_t *points0, int32_t q);
+int serve_poll(Server *s, int64_t ticket, double *out, double *times);
+int serve_wait(Server *s, int64_t ticket, double timeout_s, double *out, double *times);
+void serve_stats(Server *s, double *out, int32_t nout);
+void serve_close(Server *s);
 
 // One source's BC contribution added into d_bc_vid (device, n doubles, vid order) using only the
 // library's static device scratch; enqueued on `stream` (nullptr: the index's stream).

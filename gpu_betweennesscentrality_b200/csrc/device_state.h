@@ -1,0 +1,106 @@
+// device_state.h -- device-resident index and scratch of libqbc_b200 (internal to the library:
+// shared by the kernel drivers in device.cu and the sweep / batch / serve engine in sweep.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/qbc_b200.h"
+#include "device.h"
+
+namespace qbc {
+
+#define CK(call)                                                                                    \
+  do {                                                                                              \
+    cudaError_t e_ = (call);                                                                        \
+    if (e_ != cudaSuccess)                                                                          \
+      throw Error(e_ == cudaErrorMemoryAllocation ? QBC_ENOMEM : QBC_ECUDA,                         \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                              \
+  } while (0)
+
+enum : int32_t { ERR_NONE = 0, ERR_HOP_CAP = 1, ERR_DISCONNECTED = 2, ERR_BAD_SOURCE = 3, ERR_COPY_TIMEOUT = 4 };
+
+// ------------------------------------------------------------------------------- state
+struct SweepCache;  // captured sweep graphs (sweep.cu)
+
+struct DeviceState {
+  int device = 0;
+  cudaStream_t s_label = nullptr, s_dep = nullptr;
+  cudaEvent_t ev_label[2] = {nullptr, nullptr}, ev_dep[2] = {nullptr, nullptr}, ev_start = nullptr;
+  int32_t n = 0, n_pad = 0, hmax_pad = 0;
+  int32_t *depth = nullptr, *send = nullptr, *arc_off = nullptr, *arc_head = nullptr, *arc_w = nullptr;
+  int2 *arc_rng = nullptr, *arc_hw = nullptr;
+  int32_t *vid_of = nullptr, *tid_of = nullptr, *dis = nullptr, *anc = nullptr, *aend = nullptr;
+  int32_t packed_bits = 0;  // > 0: the packed-key label scan applies
+  int64_t *lab_off = nullptr;
+  int2 *ch = nullptr;
+  // scratch, two buffers of `chunk` slots
+  int32_t chunk = 0;
+  int2 *dc[2] = {nullptr, nullptr};
+  int32_t *hop[2] = {nullptr, nullptr};
+  double *delta[2] = {nullptr, nullptr};
+  int32_t *order[2] = {nullptr, nullptr};
+  int32_t *lcnt[2] = {nullptr, nullptr};
+  int32_t *src[2] = {nullptr, nullptr};
+  int32_t *maxhop[2] = {nullptr, nullptr};
+  double *bc_tid = nullptr;
+  double *bc_vid = nullptr;
+  int32_t *sources = nullptr;  // staging for host source lists
+  int32_t sources_cap = 0;
+  int32_t *err = nullptr;
+  int64_t bytes = 0, scratch_bytes = 0;
+  int smem_optin = 0;
+  // optional per-launch timing of the two main kernels (events on their launching streams)
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_lab, ev_dp;
+  size_t ev_lab_used = 0, ev_dp_used = 0;
+  double label_ms = 0.0, dep_ms = 0.0;
+  int64_t label_launches = 0, dep_launches = 0, launches = 0;
+  SweepCache *sweep = nullptr;
+};
+
+static std::pair<cudaEvent_t, cudaEvent_t> take_events(std::vector<std::pair<cudaEvent_t, cudaEvent_t>> &pool,
+                                                       size_t &used) {
+  if (used == pool.size()) {
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    pool.push_back({a, b});
+  }
+  return pool[used++];
+}
+
+template <class T>
+static T *dmalloc(DeviceState *d, size_t count) {
+  void *p = nullptr;
+  if (count == 0) count = 1;
+  CK(cudaMalloc(&p, count * sizeof(T)));
+  d->bytes += (int64_t)(count * sizeof(T));
+  return (T *)p;
+}
+
+template <class T>
+static T *dupload(DeviceState *d, const std::vector<T> &v, cudaStream_t s) {
+  T *p = dmalloc<T>(d, v.size());
+  if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  return p;
+}
+
+// Launches of one chunk of sources (their tids at d_src_tid, cnt <= chunk) on stream st, using
+// scratch buffer `buf`: the label scan, then the dependency pass, which adds 0.5 * delta into
+// d->bc_tid (not cleared here).  Nothing in it synchronises, so it can be stream-captured.
+void launch_chunk(const Handle &h, DeviceState *d, const int32_t *d_src_tid, int32_t cnt, int buf, cudaStream_t st);
+// out_vid[vid_of[t]] (+)= in_tid[t] for all t
+void launch_tid_to_vid(DeviceState *d, const double *in_tid, double *out_vid, int accumulate, cudaStream_t st);
+// tids of cnt vids (sets ERR_BAD_SOURCE for ids out of range)
+void launch_vid_to_tid(DeviceState *d, const int32_t *vids, int32_t *tids, int32_t cnt, cudaStream_t st);
+DeviceState *need_dev(Handle &h);
+// frees the captured sweep graphs (they hold scratch pointers; called whenever scratch changes)
+void sweep_cache_free(DeviceState *d);
+// reads and clears the device error word; throws QBC_EDEVICE when a kernel set it (synchronous)
+void check_err(DeviceState *d);
+
+}  // namespace qbc

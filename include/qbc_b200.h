@@ -90,7 +90,8 @@ int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int3
  * 1..32 forces the general kernel with 32/K sources per CTA), [1]=threads per CTA of the general
  * label kernel, [2]=target split per source group (0=auto), [3]=sources per chunk (0=auto),
  * [4]=threads per CTA of the CTA-per-source dependency kernel, [5]=dependency form (0 auto,
- * 1 one warp per source, 2 one CTA per source). */
+ * 1 one warp per source, 2 one CTA per source), [6]=level-queue depth of the warp form (layers
+ * counted in shared memory, 64..2048; 0 = 512).  Refused with QBC_EBUSY while the index serves. */
 int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams);
 int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams);
 
@@ -101,9 +102,17 @@ int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams)
 int qbc_index_profile(qbc_index *idx, int on);
 int qbc_index_stats(qbc_index *idx, double *out);
 
+/* Autotuner (no counterpart in the reference): times candidate tunings -- sources per CTA and
+ * threads of the label kernel, target split, dependency form and level-queue depth, chunk size --
+ * on a sweep over the listed sources, keeps the fastest on the index and returns it in params
+ * (layout of qbc_index_set_tuning, up to 7) with its time per source in ms. */
+int qbc_autotune(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *params, int32_t nparams,
+                 double *ms_per_source);
+
 /* ---- BC (replaces Graph::brandesBCIndexGPU_5, MHLQBC.cu:495-537 / QBC.cu:419-584) ------------
  * Batched path: many sources per launch, label rows staged in shared memory, level-bucketed
- * backprop.  bc_out: n host doubles (overwritten). */
+ * backprop.  qbc_bc_all's sweep is captured once into a CUDA graph per tuning and replayed.
+ * bc_out: n host doubles (overwritten). */
 int qbc_bc_all(qbc_index *idx, double *bc_out);
 /* partial BC over a source list (0-based vids) */
 int qbc_bc_sources(qbc_index *idx, const int32_t *sources0, int32_t ns, double *bc_out);
@@ -133,9 +142,37 @@ int qbc_bc_source_static(qbc_index *idx, int32_t source0, double *d_bc, void *st
  * BC of each query vertex over all sources (the reference's pair formula equals BC restricted to
  * the query set).  points0: q 0-based vids; out: q doubles. */
 int qbc_bc_query(qbc_index *idx, const int32_t *points0, int32_t q, double *out);
-/* many query sets sharing one source sweep: set i is points0[set_off[i] .. set_off[i+1]) */
+/* Batched RQ: many query sets sharing one source sweep (a replayed CUDA graph, as qbc_bc_all):
+ * set i is points0[set_off[i] .. set_off[i+1]), set_off[0] = 0; out has set_off[nsets] doubles.
+ * sources0 (ns vids) restricts the sweep to those sources (partial sums), NULL = all. */
 int qbc_bc_query_batch(qbc_index *idx, const int32_t *points0, const int32_t *set_off, int32_t nsets,
                        const int32_t *sources0, int32_t ns, double *out);
+
+/* ---- Served RQ (no counterpart in the reference) ------------------------------------------------
+ * A request loop on its own host thread and CUDA stream keeps sweeping the source list (NULL = all
+ * vertices) chunk by chunk while requests are in flight; each chunk's launches are one captured
+ * CUDA graph whose last kernel adds the chunk's BC into the device accumulator of every admitted
+ * request.  A request (a vertex set) is admitted at the next chunk boundary when fewer than
+ * opts[0] requests are active (default 64) and its q accumulators fit in the request pool of
+ * opts[1] bytes (16 B per query vertex; 0 = min(free device memory / 8, 64 MiB)); it completes
+ * after one full turn over the sources from its admission, so its values equal qbc_bc_query's
+ * (up to FP64 summation order) whatever else runs.  opts[2] = queue capacity (0 = 2^20).  While a
+ * server is open the index refuses every other device call with QBC_EBUSY.
+ * times (3 doubles, may be NULL) = submit, admission and completion in seconds since open. */
+typedef struct qbc_server qbc_server;
+int qbc_serve_open(qbc_index *idx, const int32_t *sources0, int32_t ns, const int64_t *opts, int32_t nopts,
+                   qbc_server **out);
+/* queues a request of q vertices (0-based vids); QBC_EBUSY when the queue is full */
+int qbc_serve_submit(qbc_server *srv, const int32_t *points0, int32_t q, int64_t *ticket);
+/* *done = 1 and out (q doubles) filled once the request is complete (the ticket is then released) */
+int qbc_serve_poll(qbc_server *srv, int64_t ticket, double *out, double *times, int32_t *done);
+/* as qbc_serve_poll, waiting up to timeout_s seconds (< 0: no limit) */
+int qbc_serve_wait(qbc_server *srv, int64_t ticket, double timeout_s, double *out, double *times, int32_t *done);
+/* out[0]=chunks run, [1]=turns over the sources, [2]=requests done, [3]=active, [4]=queued,
+ * [5]=pool entries in use, [6]=pool capacity, [7]=chunks per turn, [8]=sources per turn */
+int qbc_serve_stats(qbc_server *srv, double *out, int32_t nout);
+/* cancels queued and active requests, waits for the device work in flight, frees the server */
+int qbc_serve_close(qbc_server *srv);
 
 /* ---- per-source rows (the K2 output: MHLQBC.cu:334-412, RQ.cu:228-291, QBC.cu:272-331) ------
  * dist/cnt/hop: ns*n each, row k = source sources0[k], column = 0-based vid.  cnt and hop may be
