@@ -38,8 +38,10 @@ def _env_rank():
 
 
 def _config(n_actual, m_und, ns, args, extra=None):
-    c = {"workload": f"MHL-QBC full BC, seeded perturbed grid n={n_actual} (~{m_und} undirected edges, "
-                     f"27% lattice edges deleted, weights round(euclid*U[0.8,1.2]) in 1..1000)",
+    what = "full BC" if ns >= n_actual else f"partial BC over a seeded sample of {ns} sources"
+    sc = (f" + {args.shortcuts:.0%} random shortcut edges (weights 500..5000)" if args.shortcuts else "")
+    c = {"workload": f"MHL-QBC {what}, seeded perturbed grid n={n_actual} (~{m_und} undirected edges, "
+                     f"27% lattice edges deleted, weights round(euclid*U[0.8,1.2]) in 1..1000){sc}",
          "n": n_actual, "edges_undirected": m_und, "sources_per_step": ns, "graph_seed": args.seed,
          "parallelism": f"source-sharded x{args.gpus}" if args.gpus > 1 else "1 GPU",
          "l2": "working set (index + per-source scratch) > 126 MB L2; L2 additionally flushed between steps"}
@@ -167,32 +169,34 @@ def cpu_baseline(path, seconds=12.0):
                       f"(OpenMP over sources), {dt:.1f} s"}
 
 
-def rq_measurements(idx, n, sweep_value, args):
+def rq_measurements(idx, n, sweep_value, args, sources=None):
     """Batched RQ (64 query sets, sizes log-uniform in 16..16384, one graph-replayed sweep) against
     the plain per-set calls, and the served loop under Poisson arrivals at three rates (request sizes
     log-uniform in 1..8192).  Host-timed through the public API with host buffers."""
     from gpu_betweennesscentrality_b200.serve import poisson_load, request_sets
 
     sets = request_sets(n, 64, 16, 16384, seed=2)
-    idx.bc_query_batch(sets)  # capture + warm
+    ns = n if sources is None else int(len(sources))
+    idx.bc_query_batch(sets, sources=sources)  # capture + warm
     reps = 3
     t = time.perf_counter()
     for _ in range(reps):
-        outs = idx.bc_query_batch(sets)
+        outs = idx.bc_query_batch(sets, sources=sources)
     t_batch = (time.perf_counter() - t) / reps
     k_plain = 4  # 64 sequential per-set sweeps would take 64 sweeps; 4 of them are timed
     t = time.perf_counter()
-    plain_outs = [idx.bc_query(s) for s in sets[:k_plain]]
+    plain_outs = [idx.bc_query(s) if sources is None else idx.bc_query_batch([s], sources=sources)[0]
+                  for s in sets[:k_plain]]
     t_plain_set = (time.perf_counter() - t) / k_plain
     diff = max(float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) for a, b in zip(outs, plain_outs))
     batched = {"max_rel_diff_vs_plain": diff, "sets": 64, "query_vertices": int(sum(len(s) for s in sets)), "ms": t_batch * 1e3,
-               "sources_per_s": 64 * n / t_batch,
-               "plain_per_set_ms": t_plain_set * 1e3, "plain_sources_per_s": n / t_plain_set,
+               "sources_per_s": 64 * ns / t_batch,
+               "plain_per_set_ms": t_plain_set * 1e3, "plain_sources_per_s": ns / t_plain_set,
                "speedup_vs_64_sequential": 64 * t_plain_set / t_batch,
                "note": f"plain = one qbc_bc_query call (one full sweep) per set, {k_plain} of 64 timed; "
                        "batched = one qbc_bc_query_batch call, one graph-replayed sweep for all 64 sets"}
     # served: slots = 64 concurrent requests; one turn over the sources takes n / sweep rate
-    turn_s = n / sweep_value
+    turn_s = ns / sweep_value
     slots = 64
     capacity = slots / turn_s
     served = {"slots": slots, "turn_ms": turn_s * 1e3, "capacity_requests_per_s": capacity, "rates": []}
@@ -200,7 +204,7 @@ def rq_measurements(idx, n, sweep_value, args):
         rate = frac * capacity
         count = max(20, int(rate * args.served_seconds))
         reqs = request_sets(n, count, 1, 8192, seed=100 + i)
-        with idx.serve(max_active=slots) as srv:
+        with idx.serve(sources=sources, max_active=slots) as srv:
             r = poisson_load(srv, reqs, rate=rate, seed=3 + i)
         r["rate_fraction_of_capacity"] = frac
         served["rates"].append({k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()})
@@ -218,6 +222,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=0, help="sources per scratch buffer (0: sized from free HBM)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default tuning instead of autotuning")
+    ap.add_argument("--sample", type=int, default=0,
+                    help="sources per step: a seeded sample of this many vertices (0: all n, the full BC)")
+    ap.add_argument("--shortcuts", type=float, default=0.0, help="fraction of n random shortcut edges (500..5000)")
     ap.add_argument("--no-rq", action="store_true", help="skip the batched and served RQ measurements")
     ap.add_argument("--served-seconds", type=float, default=8.0, help="arrival window per served rate")
     args = ap.parse_args()
@@ -242,10 +249,10 @@ def main():
     dev = torch.device("cuda", local)
 
     if rank == 0:
-        path = synth.cached_graph(CACHE, args.n, seed=args.seed)
+        path = synth.cached_graph(CACHE, args.n, seed=args.seed, shortcut_frac=args.shortcuts)
     if world > 1:
         dist.barrier(device_ids=[local])
-    path = synth.cached_graph(CACHE, args.n, seed=args.seed)
+    path = synth.cached_graph(CACHE, args.n, seed=args.seed, shortcut_frac=args.shortcuts)
 
     G = q.Graph(device=local)
     t = time.perf_counter()
@@ -263,10 +270,17 @@ def main():
     info = idx.info()
     n = G.nodenum
     ex_vid = idx.export()["vid_of"]  # tid order keeps each CTA's sources close in the tree
+    if args.sample and args.sample < n:
+        # a seeded sample of sources, kept in tid order
+        tid_of = np.empty(n, np.int64)
+        tid_of[ex_vid] = np.arange(n)
+        pick = np.random.default_rng(args.seed + 1).choice(n, args.sample, replace=False)
+        ex_vid = ex_vid[np.sort(tid_of[pick])]
+    n_sources = int(ex_vid.shape[0])
     tune = None
     if not args.no_autotune and not args.chunk:
         t = time.perf_counter()
-        sample = ex_vid[:: max(1, n // 8192)][:8192]
+        sample = ex_vid[:: max(1, n_sources // 8192)][:8192]
         tune = idx.autotune(sample)
         tune["seconds"] = round(time.perf_counter() - t, 2)
     from gpu_betweennesscentrality_b200.shard import all_reduce_bc, max_over_ranks, shard_sources
@@ -309,7 +323,7 @@ def main():
         ms = max_over_ranks(ms, device=dev)
         all_reduce_bc(d_bc)  # the one exchange: sum of the ranks' partial BC vectors
         torch.cuda.synchronize()
-    value = n * args.steps / (ms / 1e3)
+    value = n_sources * args.steps / (ms / 1e3)
 
     # end to end through the C-ABI call with pinned host buffers: H2D of the source list and D2H of BC
     h_src = torch.from_numpy(shard).pin_memory()
@@ -324,7 +338,7 @@ def main():
     e2e_s = time.perf_counter() - t
     if world > 1:
         e2e_s = max_over_ranks(e2e_s, device=dev)
-    e2e_val = n * e2e_steps / e2e_s
+    e2e_val = n_sources * e2e_steps / e2e_s
 
     # Roofline of the dominant kernel (the label scan).  Algorithmic bytes follow the per-source
     # label term of the workload's byte model: 12 B (dist, count, hop) per label entry a scan
@@ -347,7 +361,7 @@ def main():
     achieved = per_launch_bytes / (per_launch_ms / 1e3) / 1e9
     traffic = None
     prof = os.path.join(ROOT, "profiles", "k_label_scan_packed_50k.md")
-    if os.path.exists(prof):
+    if os.path.exists(prof) and args.n == 50000 and not args.shortcuts and n_sources == n:
         import re
         m = re.search(r"dram_bytes_per_source:\s*([0-9.e+]+)", open(prof).read())
         if m:
@@ -367,7 +381,7 @@ def main():
                            f"dependency launch each, host-timed with the final synchronisation"}
     rq = None
     if rank == 0 and world == 1 and not args.no_rq:
-        rq = rq_measurements(idx, n, value, args)
+        rq = rq_measurements(idx, n, value, args, None if n_sources == n else ex_vid)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(path)
@@ -376,7 +390,7 @@ def main():
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                "scaling": "strong", "vs_baseline": None,
                "dtype": "int32 dist / uint32 wrapping count / int32 hop; f64 dependency", "data": "synthetic",
-               "config": _config(n, int(info[1]) // 2, n, args,
+               "config": _config(n, int(info[1]) // 2, n_sources, args,
                                  {"index": {"tree_height": int(info[3]), "tree_width": int(info[4]),
                                             "label_entries": int(info[7]), "device_bytes": int(info[5]),
                                             "host_build_s": round(t_build, 3), "read_s": round(t_read, 3),

@@ -124,25 +124,28 @@ class Index:
         check(lib().qbc_index_scan_entries(self.h, ptr(s, i32p), int(s.shape[0]), C.byref(e)))
         return int(e.value)
 
-    TUNING_KEYS = ("lanes_per_source", "label_threads", "split", "chunk", "dep_threads", "dep_form", "queue_depth")
+    TUNING_KEYS = ("lanes_per_source", "label_threads", "split", "chunk", "dep_threads", "dep_form", "queue_depth",
+                   "label_warps", "label_tile")
 
     def set_tuning(self, lanes_per_source=0, label_threads=256, split=0, chunk=0, dep_threads=256, dep_form=0,
-                   queue_depth=0):
-        p = i32([lanes_per_source, label_threads, split, chunk, dep_threads, dep_form, queue_depth])
-        check(lib().qbc_index_set_tuning(self.h, ptr(p, i32p), 7))
+                   queue_depth=0, label_warps=0, label_tile=0):
+        p = i32([lanes_per_source, label_threads, split, chunk, dep_threads, dep_form, queue_depth, label_warps,
+                 label_tile])
+        check(lib().qbc_index_set_tuning(self.h, ptr(p, i32p), len(self.TUNING_KEYS)))
 
     def get_tuning(self):
-        p = np.zeros(7, np.int32)
-        check(lib().qbc_index_get_tuning(self.h, ptr(p, i32p), 7))
+        p = np.zeros(len(self.TUNING_KEYS), np.int32)
+        check(lib().qbc_index_get_tuning(self.h, ptr(p, i32p), len(self.TUNING_KEYS)))
         return dict(zip(self.TUNING_KEYS, p.tolist()))
 
     def autotune(self, sample, path: Optional[str] = None) -> dict:
         """Times candidate tunings on a sweep over ``sample`` (vids), keeps the fastest on the index
         and returns it; with ``path`` it is also written there as JSON (``load_tuning`` reads it)."""
         s = i32(sample)
-        p = np.zeros(7, np.int32)
+        p = np.zeros(len(self.TUNING_KEYS), np.int32)
         ms = C.c_double()
-        check(lib().qbc_autotune(self.h, ptr(s, i32p), int(s.shape[0]), ptr(p, i32p), 7, C.byref(ms)))
+        check(lib().qbc_autotune(self.h, ptr(s, i32p), int(s.shape[0]), ptr(p, i32p), len(self.TUNING_KEYS),
+                                 C.byref(ms)))
         res = dict(tuning=dict(zip(self.TUNING_KEYS, p.tolist())), ms_per_source=float(ms.value),
                    sample_sources=int(s.shape[0]), n=self.n)
         if path:

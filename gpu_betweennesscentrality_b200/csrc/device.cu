@@ -283,13 +283,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   return false;
 }
 
-constexpr int kPackedThreads = 512;
-constexpr int kPackedWarps = kPackedThreads / 32;
 constexpr int kRowBuffers = 2;  // per-warp target-row buffers: 1 copy in flight
 constexpr int kStageInt4 = 32 * 5 + 32 * 3;  // per-warp output staging (int4s)
 
-template <bool COUNTS>
-__global__ void __launch_bounds__(kPackedThreads, 1) k_label_scan_packed(LabelArgs a) {
+// Shared memory of the packed kernel with `warps` warps and row stride S (entries): 32 source key
+// rows, kRowBuffers target rows per warp, per-warp output staging.
+__host__ __device__ constexpr size_t packed_smem(int warps, int S) {
+  return (size_t)32 * S * 4 + (size_t)warps * (kRowBuffers * (size_t)S * 4 + kStageInt4 * 16);
+}
+
+// Rows are held in shared memory up to S entries (S = the padded tree height when it fits);
+// entries j >= S of a scan (taller trees) are read from global memory, 4 at a time.
+template <bool COUNTS, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a) {
   constexpr int G = 32;
   extern __shared__ int4 smem4[];
   uint32_t *s_key = reinterpret_cast<uint32_t *>(smem4);
@@ -302,7 +308,7 @@ __global__ void __launch_bounds__(kPackedThreads, 1) k_label_scan_packed(LabelAr
   int32_t *shp1 = reinterpret_cast<int32_t *>(shp) + lane * 12;  // this lane's 8 hop layers
   __shared__ int32_t s_h[G];
   __shared__ int64_t s_off[G];
-  __shared__ __align__(8) uint64_t s_bar[kPackedWarps][kRowBuffers];
+  __shared__ __align__(8) uint64_t s_bar[WARPS][kRowBuffers];
   const int first = blockIdx.y * G;
   if (first >= a.ns) return;
   const int gcount = min(G, a.ns - first);
@@ -320,7 +326,7 @@ __global__ void __launch_bounds__(kPackedThreads, 1) k_label_scan_packed(LabelAr
   for (int idx = threadIdx.x; idx < G * S; idx += blockDim.x) {
     const int i = idx / S, j = idx - i * S;
     uint32_t key = 0xffffffffu;
-    if (i < gcount && j < s_h[i]) key = ((uint32_t)a.dis[s_off[i] + j] << B) | (uint32_t)j;
+    if (i < gcount && j < s_h[i]) key = ((uint32_t)a.dis[s_off[i] + j] << B) | (uint32_t)j;  // j < S
     s_key[idx] = key;
   }
   __syncthreads();
@@ -346,7 +352,7 @@ __global__ void __launch_bounds__(kPackedThreads, 1) k_label_scan_packed(LabelAr
     if (t >= a.n) { next_c = cend; return; }
     if (lane == 0) {
       const uint32_t b = issued % kRowBuffers;
-      const uint32_t bytes = (uint32_t)(((a.depth[t] + 3) & ~3) * 4);
+      const uint32_t bytes = (uint32_t)(min((a.depth[t] + 3) & ~3, S) * 4);  // S is a multiple of 4
       bulk_row_to_smem(tb0 + b * S, a.dis + a.lab_off[t], bytes, &s_bar[warp][b]);
     }
     issued++;
@@ -396,8 +402,9 @@ __global__ void __launch_bounds__(kPackedThreads, 1) k_label_scan_packed(LabelAr
       done++;
       const int32_t *tbuf = tb0 + b * S;
       const int hl = have ? J + 1 : 0;
+      const int hm = min(hl, S);  // entries held in shared memory
       uint32_t m1 = 0xffffffffu, m2 = 0xffffffffu, n1 = 0xffffffffu, n2 = 0xffffffffu;
-      const int full8 = hl & ~7;
+      const int full8 = hm & ~7;
       int j = 0;
       for (; j < full8; j += 8) {
         const uint4 x = *reinterpret_cast<const uint4 *>(srow + j);
@@ -416,13 +423,26 @@ __global__ void __launch_bounds__(kPackedThreads, 1) k_label_scan_packed(LabelAr
         m2 = __vimin3_u32(m2, v2 ^ mask, v3 ^ mask);
         n2 = __vimin3_u32(n2, u2 ^ mask, u3 ^ mask);
       }
-      for (; j < hl; j += 4) {
+      for (; j < hm; j += 4) {
         const uint4 x = *reinterpret_cast<const uint4 *>(srow + j);
         const uint4 y = *reinterpret_cast<const uint4 *>(tbuf + j);
         const uint32_t v0 = x.x + (y.x << B);
-        const uint32_t v1 = (j + 1 < hl) ? x.y + (y.y << B) : 0xffffffffu;
-        const uint32_t v2 = (j + 2 < hl) ? x.z + (y.z << B) : 0xffffffffu;
-        const uint32_t v3 = (j + 3 < hl) ? x.w + (y.w << B) : 0xffffffffu;
+        const uint32_t v1 = (j + 1 < hm) ? x.y + (y.y << B) : 0xffffffffu;
+        const uint32_t v2 = (j + 2 < hm) ? x.z + (y.z << B) : 0xffffffffu;
+        const uint32_t v3 = (j + 3 < hm) ? x.w + (y.w << B) : 0xffffffffu;
+        m1 = __vimin3_u32(m1, v0, v1);
+        m1 = __vimin3_u32(m1, v2, v3);
+        m2 = __vimin3_u32(m2, v0 ^ mask, (j + 1 < hm) ? v1 ^ mask : 0xffffffffu);
+        m2 = __vimin3_u32(m2, (j + 2 < hm) ? v2 ^ mask : 0xffffffffu, (j + 3 < hm) ? v3 ^ mask : 0xffffffffu);
+      }
+      const int64_t toff_t = (hl > S) ? a.lab_off[t] : 0;
+      for (j = S; j < hl; j += 4) {  // beyond the shared rows: both rows from global memory
+        const uint4 x = __ldg(reinterpret_cast<const uint4 *>(a.dis + soff + j));
+        const uint4 y = __ldg(reinterpret_cast<const uint4 *>(a.dis + toff_t + j));
+        const uint32_t v0 = (((uint32_t)x.x + (uint32_t)y.x) << B) | (uint32_t)j;
+        const uint32_t v1 = (j + 1 < hl) ? ((((uint32_t)x.y + (uint32_t)y.y) << B) | (uint32_t)(j + 1)) : 0xffffffffu;
+        const uint32_t v2 = (j + 2 < hl) ? ((((uint32_t)x.z + (uint32_t)y.z) << B) | (uint32_t)(j + 2)) : 0xffffffffu;
+        const uint32_t v3 = (j + 3 < hl) ? ((((uint32_t)x.w + (uint32_t)y.w) << B) | (uint32_t)(j + 3)) : 0xffffffffu;
         m1 = __vimin3_u32(m1, v0, v1);
         m1 = __vimin3_u32(m1, v2, v3);
         m2 = __vimin3_u32(m2, v0 ^ mask, (j + 1 < hl) ? v1 ^ mask : 0xffffffffu);
@@ -441,7 +461,9 @@ __global__ void __launch_bounds__(kPackedThreads, 1) k_label_scan_packed(LabelAr
           unsigned cc = 0;
           int hh = 0;
           for (int q = 0; q < hl; q++) {
-            if (((srow[q] + ((uint32_t)tbuf[q] << B)) >> B) == dist) {
+            const uint32_t dq = q < S ? (srow[q] + ((uint32_t)tbuf[q] << B)) >> B
+                                      : (uint32_t)(__ldg(a.dis + soff + q) + __ldg(a.dis + toff + q));
+            if (dq == dist) {
               const int2 cs = __ldg(a.ch + soff + q), ct = __ldg(a.ch + toff + q);
               cc += (unsigned)cs.x * (unsigned)ct.x;
               hh = max(hh, cs.y + ct.y);
@@ -971,31 +993,53 @@ static void launch_label_c(const LabelPlan &p, const LabelArgs &a, int groups, c
   }
 }
 
-template <bool C>
-static void launch_label_packed(const Handle &h, const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
-  constexpr int threads = kPackedThreads;
-  const int S = d->hmax_pad;
-  const size_t smem = (size_t)32 * S * 4 + (size_t)(threads / 32) * (kRowBuffers * S * 4 + kStageInt4 * 16);
+// Row stride of the packed kernel with `warps` warps: the padded tree height when it fits the
+// shared memory (and the tuned label tile), else the largest fitting stride (multiple of 4
+// entries, odd in 16-byte units).
+static int packed_stride(const Handle &h, const DeviceState *d, int warps) {
+  const size_t budget = (size_t)std::max(0, d->smem_optin - 2048);
+  int S = d->hmax_pad;
+  if (h.tuning.label_tile > 0) S = std::min(S, std::max(8, (h.tuning.label_tile + 3) & ~3));
+  while (S > 8 && packed_smem(warps, S) > budget) S -= 4;
+  if (((S / 4) & 1) == 0) S -= 4;
+  return S;
+}
+
+// 16 warps when the whole tree height fits, else 8 warps (twice the rows per CTA); or as tuned
+static int packed_warps(const Handle &h, const DeviceState *d) {
+  if (h.tuning.label_warps == 8 || h.tuning.label_warps == 16) return h.tuning.label_warps;
+  return packed_stride(h, d, 16) >= d->hmax_pad ? 16 : 8;
+}
+
+template <bool C, int W>
+static void launch_label_packed_w(const Handle &h, const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
+  const int S = packed_stride(h, d, W);
+  const size_t smem = packed_smem(W, S);
   const int groups = (ns + 31) / 32;
   int split = h.tuning.split;
   if (split <= 0) {
     split = std::max(1, (148 * 4 + groups - 1) / groups);
-    split = std::min(split, std::max(1, (d->n_pad / 8) / (threads / 32)));
+    split = std::min(split, std::max(1, (d->n_pad / 8) / W));
   }
   a.stride = S;
   a.split = split;
-  auto kern = k_label_scan_packed<C>;
+  auto kern = k_label_scan_packed<C, W>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(split, groups);
-  kern<<<grid, threads, smem, st>>>(a);
+  kern<<<grid, W * 32, smem, st>>>(a);
   CK(cudaGetLastError());
 }
 
+template <bool C>
+static void launch_label_packed(const Handle &h, const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
+  if (packed_warps(h, d) == 16) launch_label_packed_w<C, 16>(h, d, a, ns, st);
+  else launch_label_packed_w<C, 8>(h, d, a, ns, st);
+}
+
+// the packed-key kernel applies when its keys fit 32 bits
 static bool use_packed(const Handle &h, const DeviceState *d, bool plain) {
-  if (plain || d->packed_bits == 0) return false;
-  const int k = h.tuning.lanes_per_source;
-  const size_t smem = (size_t)(32 + kRowBuffers * kPackedWarps) * d->hmax_pad * 4 + (size_t)kPackedWarps * kStageInt4 * 16;
-  return k == 0 && smem + 2048 <= (size_t)d->smem_optin;
+  if (plain || d->packed_bits == 0 || h.tuning.lanes_per_source != 0) return false;
+  return packed_stride(h, d, packed_warps(h, d)) >= 8 && packed_smem(8, 8) <= (size_t)d->smem_optin;
 }
 
 static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t *src, int32_t ns, bool plain,
@@ -1062,10 +1106,13 @@ static DepArgs dep_args(DeviceState *d, int buf, const int32_t *src, int32_t ns)
   return a;
 }
 
-static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *src, int32_t ns, cudaStream_t st) {
+// plain = a single source: one CTA runs its dependency pass (the warp form would leave 7/8 of the
+// CTA idle)
+static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *src, int32_t ns, cudaStream_t st,
+                       bool plain = false) {
   DepArgs a = dep_args(d, buf, src, ns);
   const int threads = std::max(64, std::min(256, (h.tuning.dep_threads / 32) * 32));
-  const bool warp_form = h.host.kind == IndexKind::MHL && h.tuning.dep_form != 2;
+  const bool warp_form = h.host.kind == IndexKind::MHL && h.tuning.dep_form != 2 && !plain;
   std::pair<cudaEvent_t, cudaEvent_t> ev{};
   if (d->profiling) {
     ev = take_events(d->ev_dp, d->ev_dp_used);
@@ -1372,7 +1419,7 @@ void host_bc_plain(Handle &h, const int32_t *sources0, int32_t ns, double *bc_ou
     k_vid_to_tid<<<1, 32, 0, st>>>(ds + i, d->tid_of, d->src[0], 1, d->n, d->err);
     CK(cudaGetLastError());
     launch_label(h, d, 0, d->src[0], 1, true, st);
-    launch_dep(h, d, 0, d->src[0], 1, st);
+    launch_dep(h, d, 0, d->src[0], 1, st, true);
   }
   k_tid_to_vid_f64<<<(d->n + 255) / 256, 256, 0, st>>>(d->bc_tid, d->vid_of, d->bc_vid, d->n, 0);
   CK(cudaGetLastError());

@@ -60,7 +60,7 @@ uint64_t fnv(uint64_t h, const void *p, size_t bytes) {
 
 uint64_t tuning_key(const Handle &h, const DeviceState *d) {
   const Tuning &t = h.tuning;
-  const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.dep_threads, t.dep_form, t.queue_depth, d->chunk};
+  const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, d->chunk};
   return fnv(1469598103934665603ull, f, sizeof(f));
 }
 
@@ -313,11 +313,18 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
       }
     };
     best.chunk = d->chunk;
-    // 1. sources per CTA and threads of the label kernel (0 = packed-key kernel where it applies)
-    for (int32_t lanes : {0, 4, 8, 16})
+    // 1. label kernel: the packed-key kernel with 8 or 16 warps (0 lanes), or the general kernel
+    //    with 32/K sources per CTA and 128 or 256 threads
+    if (d->packed_bits)
+      for (int32_t warps : {8, 16}) {
+        Tuning t = best;
+        t.lanes_per_source = 0;
+        t.label_warps = warps;
+        trial(t);
+      }
+    for (int32_t lanes : {4, 8, 16})
       for (int32_t threads : {128, 256}) {
-        if (lanes == 0 && threads == 128) continue;
-        if (lanes > 0 && !label_fits(h, d, lanes, threads)) continue;
+        if (!label_fits(h, d, lanes, threads)) continue;
         Tuning t = best;
         t.lanes_per_source = lanes;
         t.label_threads = threads;

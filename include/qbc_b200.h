@@ -91,7 +91,10 @@ int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int3
  * label kernel, [2]=target split per source group (0=auto), [3]=sources per chunk (0=auto),
  * [4]=threads per CTA of the CTA-per-source dependency kernel, [5]=dependency form (0 auto,
  * 1 one warp per source, 2 one CTA per source), [6]=level-queue depth of the warp form (layers
- * counted in shared memory, 64..2048; 0 = 512).  Refused with QBC_EBUSY while the index serves. */
+ * counted in shared memory, 64..2048; 0 = 512), [7]=warps per CTA of the packed-key kernel (8 or
+ * 16; 0 = 16 when the whole tree height fits shared memory, else 8), [8]=label tile: entries of
+ * each row staged in shared memory by the packed-key kernel (0 = all that fit; later entries of a
+ * scan are read from global memory).  Refused with QBC_EBUSY while the index serves. */
 int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams);
 int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams);
 
@@ -105,7 +108,7 @@ int qbc_index_stats(qbc_index *idx, double *out);
 /* Autotuner (no counterpart in the reference): times candidate tunings -- sources per CTA and
  * threads of the label kernel, target split, dependency form and level-queue depth, chunk size --
  * on a sweep over the listed sources, keeps the fastest on the index and returns it in params
- * (layout of qbc_index_set_tuning, up to 7) with its time per source in ms. */
+ * (layout of qbc_index_set_tuning, up to 9) with its time per source in ms. */
 int qbc_autotune(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *params, int32_t nparams,
                  double *ms_per_source);
 
@@ -116,7 +119,8 @@ int qbc_autotune(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *p
 int qbc_bc_all(qbc_index *idx, double *bc_out);
 /* partial BC over a source list (0-based vids) */
 int qbc_bc_sources(qbc_index *idx, const int32_t *sources0, int32_t ns, double *bc_out);
-/* plain path: one source per launch sequence (label kernel, then dependency kernel) */
+/* plain path: one source per launch sequence (label kernel over the whole GPU, then one CTA for its
+ * dependency pass, as the reference gives each source one block, MHLQBC.cu:237-475) */
 int qbc_bc_plain(qbc_index *idx, const int32_t *sources0, int32_t ns, double *bc_out);
 /* Device-resident variant: d_sources0 (ns int32) and d_bc (n doubles, accumulated into, not
  * cleared) are device pointers; stream is a cudaStream_t or NULL for the index's own stream.

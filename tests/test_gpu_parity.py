@@ -59,6 +59,23 @@ def test_rows_identical_across_tunings(g2k, lanes):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("warps,tile", [(16, 0), (8, 0), (16, 32), (8, 48), (16, 8)])
+def test_packed_kernel_tiles_and_warps(g2k, warps, tile):
+    """label entries beyond the shared-memory tile come from global memory: same rows, same BC"""
+    n, u, v, w, g, idx, tc, arcs = g2k
+    srcs = np.arange(0, n, 11, dtype=np.int32)
+    base = idx.rows(srcs)
+    idx.set_tuning(label_warps=warps, label_tile=tile)
+    try:
+        alt = idx.rows(srcs)
+        bc = idx.bc_sources(srcs)
+    finally:
+        idx.set_tuning()
+    for a, b in zip(base, alt):
+        assert np.array_equal(a, b)
+    assert rel_err(bc, tc.bc(arcs, srcs)) <= BC_RTOL
+
+
 def test_bc_all_2k_matches_oracle_and_reference(g2k):
     n, u, v, w, g, idx, tc, arcs = g2k
     bc = idx.bc_all()
