@@ -199,12 +199,14 @@ def rq_measurements(idx, n, sweep_value, args, sources=None):
     turn_s = ns / sweep_value
     slots = 64
     capacity = slots / turn_s
-    served = {"slots": slots, "turn_ms": turn_s * 1e3, "capacity_requests_per_s": capacity, "rates": []}
+    chunk = max(256, (ns // 8 + 31) // 32 * 32)  # about 8 admission points per turn
+    served = {"slots": slots, "turn_ms": turn_s * 1e3, "capacity_requests_per_s": capacity,
+              "chunk_sources": min(chunk, idx.get_tuning()["chunk"] or chunk), "rates": []}
     for i, frac in enumerate((0.5, 0.8, 0.95)):
         rate = frac * capacity
         count = max(20, int(rate * args.served_seconds))
         reqs = request_sets(n, count, 1, 8192, seed=100 + i)
-        with idx.serve(sources=sources, max_active=slots) as srv:
+        with idx.serve(sources=sources, max_active=slots, chunk=chunk) as srv:
             r = poisson_load(srv, reqs, rate=rate, seed=3 + i)
         r["rate_fraction_of_capacity"] = frac
         served["rates"].append({k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()})
@@ -225,6 +227,8 @@ def main():
     ap.add_argument("--sample", type=int, default=0,
                     help="sources per step: a seeded sample of this many vertices (0: all n, the full BC)")
     ap.add_argument("--shortcuts", type=float, default=0.0, help="fraction of n random shortcut edges (500..5000)")
+    ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
+                    help="set a tuning field (Index.TUNING_KEYS) instead of autotuning it; repeatable")
     ap.add_argument("--no-rq", action="store_true", help="skip the batched and served RQ measurements")
     ap.add_argument("--served-seconds", type=float, default=8.0, help="arrival window per served rate")
     args = ap.parse_args()
@@ -261,8 +265,10 @@ def main():
     t = time.perf_counter()
     idx = G.build_index(upload=False)
     t_build = time.perf_counter() - t
-    if args.chunk:
-        idx.set_tuning(chunk=args.chunk)
+    if args.chunk or args.tune:
+        fixed = {"chunk": args.chunk}
+        fixed.update({k: int(v) for k, v in (t.split("=", 1) for t in args.tune)})
+        idx.set_tuning(**fixed)
     t = time.perf_counter()
     idx.upload(local)
     torch.cuda.synchronize()
@@ -278,9 +284,10 @@ def main():
         ex_vid = ex_vid[np.sort(tid_of[pick])]
     n_sources = int(ex_vid.shape[0])
     tune = None
-    if not args.no_autotune and not args.chunk:
+    if not args.no_autotune and not args.chunk and not args.tune:
         t = time.perf_counter()
-        sample = ex_vid[:: max(1, n_sources // 8192)][:8192]
+        k = int(min(8192, max(512, 8192 * 50000 / n)))  # about 50 ms of sweep per trial
+        sample = ex_vid[:: max(1, n_sources // k)][:k]
         tune = idx.autotune(sample)
         tune["seconds"] = round(time.perf_counter() - t, 2)
     from gpu_betweennesscentrality_b200.shard import all_reduce_bc, max_over_ranks, shard_sources

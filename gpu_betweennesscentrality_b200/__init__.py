@@ -159,11 +159,11 @@ class Index:
         self.set_tuning(**{k: int(t[k]) for k in self.TUNING_KEYS if k in t})
         return self.get_tuning()
 
-    def serve(self, sources=None, max_active: int = 64, pool_bytes: int = 0, max_queue: int = 0):
+    def serve(self, sources=None, max_active: int = 64, pool_bytes: int = 0, max_queue: int = 0, chunk: int = 0):
         """Opens the served RQ loop on this index (see ``serve.Server``)."""
         from .serve import Server
 
-        return Server(self, sources, max_active, pool_bytes, max_queue)
+        return Server(self, sources, max_active, pool_bytes, max_queue, chunk)
 
     def profile(self, on: bool = True) -> None:
         check(lib().qbc_index_profile(self.h, 1 if on else 0))

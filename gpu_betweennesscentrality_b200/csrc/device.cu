@@ -18,9 +18,9 @@
 //   k_kahn_dependency (QBC) distance-only rows from the H2H index; sigma and topological waves
 //                  by a device Kahn pass (QBC.cu:485-555 ran it on the host), then the same backprop.
 //
-// Chunks of sources alternate between two scratch buffers; the label scan and the dependency pass
-// of a chunk run back to back on one stream (concurrent on two streams they thrash each other's
-// caches: measured ~2x slower in total).
+// Chunks of sources run through one scratch buffer; the label scan and the dependency pass of a
+// chunk run back to back on one stream (concurrent on two streams they thrash each other's caches:
+// measured ~2x slower in total).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -63,7 +63,7 @@ struct LabelArgs {
   const int32_t *__restrict__ send;
   const int32_t *__restrict__ src;  // tids of this chunk's sources
   int32_t ns, n, n_pad, stride, split;
-  int2 *__restrict__ out_dc;      // [ns][n_pad] (dist, count bits)
+  int4 *__restrict__ out_rec;     // [ns][n_pad] records (dist, count bits, delta as f64 = 0)
   int32_t *__restrict__ out_hop;  // [ns][n_pad]
   int32_t *__restrict__ maxhop;   // [ns] largest hop layer per source (atomicMax), or null
   const int32_t *__restrict__ aend;  // subtree end of each row entry's ancestor (packed kernel)
@@ -233,11 +233,9 @@ __global__ void __launch_bounds__(256, 1) k_label_scan(LabelArgs a) {
         for (int k = 0; k < 8; k++) mh = max(mh, rh[k]);
         atomicMax(a.maxhop + slot, mh);
       }
-      int4 *od = reinterpret_cast<int4 *>(a.out_dc + blk((int)slot, t0, a.ns));
-      od[0] = make_int4(rd[0], rc[0], rd[1], rc[1]);
-      od[1] = make_int4(rd[2], rc[2], rd[3], rc[3]);
-      od[2] = make_int4(rd[4], rc[4], rd[5], rc[5]);
-      od[3] = make_int4(rd[6], rc[6], rd[7], rc[7]);
+      int4 *od = a.out_rec + blk((int)slot, t0, a.ns);
+#pragma unroll
+      for (int k = 0; k < 8; k++) od[k] = make_int4(rd[k], rc[k], 0, 0);
       if (COUNTS) {
         int4 *oh = reinterpret_cast<int4 *>(a.out_hop + blk((int)slot, t0, a.ns));
         oh[0] = make_int4(rh[0], rh[1], rh[2], rh[3]);
@@ -510,8 +508,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
     }
     __syncwarp();
     {  // the warp's 32 slots x 8 targets are one contiguous block: coalesced 512-byte stores
-      int4 *gdc = reinterpret_cast<int4 *>(a.out_dc + blk(first, t0, a.ns));
-      for (int p = lane; p < gcount * 4; p += 32) gdc[p] = sdc[(p >> 2) * 5 + (p & 3)];
+      int4 *grec = a.out_rec + blk(first, t0, a.ns);  // 16-byte records: 512 B per store instruction
+      const int2 *sdc_all = reinterpret_cast<const int2 *>(sdc);
+      for (int p = lane; p < gcount * 8; p += 32) {
+        const int2 x = sdc_all[(p >> 3) * 10 + (p & 7)];
+        grec[p] = make_int4(x.x, x.y, 0, 0);
+      }
       if (COUNTS) {
         int4 *ghp = reinterpret_cast<int4 *>(a.out_hop + blk(first, t0, a.ns));
         for (int p = lane; p < gcount * 2; p += 32) ghp[p] = shp[(p >> 1) * 3 + (p & 1)];
@@ -540,9 +542,8 @@ struct DepArgs {
   const int32_t *__restrict__ arc_w;
   const int32_t *__restrict__ src;
   int32_t ns, n, n_pad;
-  int2 *dc;        // [ns][n_pad] (dist, sigma); sigma written by the Kahn kernel
+  int4 *rec;       // [ns][n_pad] records (dist, sigma, delta as f64); sigma written by the Kahn kernel
   int32_t *hop;    // [ns][n_pad] layer (MHL) / indegree then wave (H2H)
-  double *delta;   // [ns][n_pad]
   int32_t *order;  // [ns][n_pad] level queue
   int32_t *lcnt;   // [ns][2*(n_pad+2)] global layer counters when shared ones do not suffice
   double *bc;      // [n] tid order, FP64 red target
@@ -616,31 +617,36 @@ __device__ __forceinline__ int agg_inc(int *ctr, int key, unsigned act) {
   return base + rank;
 }
 
+// A vertex's per-source record is 16 bytes: (dist, sigma bits, delta as f64), so one load brings
+// everything the backprop needs about a DAG successor.  Records are read with plain (coherent)
+// loads: delta is written during the pass.
+__device__ __forceinline__ double rec_delta(const int4 r) { return __hiloint2double(r.w, r.z); }
+__device__ __forceinline__ void set_delta(int4 *r, double d) { reinterpret_cast<double *>(r)[1] = d; }
+
 // Pull-form dependency of vertex v (MHLQBC.cu:452-466): delta(v) = sum over DAG arcs v->w of
 // sigma_v * (1 + delta_w) / sigma_w, operation order as the reference (:457).
-template <class DC>
-__device__ __forceinline__ double pull_delta(const DepArgs &a, const DC &dc, const double *delta, int v) {
-  const int2 dv = dc[v];
-  const double sv = (double)dv.y;
+template <class RV>
+__device__ __forceinline__ double pull_delta(const DepArgs &a, const RV &rec, int v) {
+  const int4 rv = rec[v];
+  const double sv = (double)rv.y;
   double acc = 0.0;
   const int e1 = a.arc_off[v + 1];
   for (int e = a.arc_off[v]; e < e1; e++) {
     const int w = a.arc_head[e];
-    const int2 dw = dc[w];
-    if (dw.x == dv.x + a.arc_w[e]) acc += sv * (1.0 + delta[w]) / (double)dw.y;
+    const int4 rw = rec[w];
+    if (rw.x == rv.x + a.arc_w[e]) acc += sv * (1.0 + rec_delta(rw)) / (double)rw.y;
   }
   return acc;
 }
 
-template <class DC>
-__device__ void backprop_levels(const DepArgs &a, const DC &dc, double *delta, const int32_t *order,
-                                const int *start, int maxL) {
+template <class RV>
+__device__ void backprop_levels(const DepArgs &a, const RV &rec, const int32_t *order, const int *start, int maxL) {
   for (int L = maxL; L >= 1; --L) {
     const int b = start[L], e = start[L + 1];
     for (int idx = b + threadIdx.x; idx < e; idx += blockDim.x) {
       const int v = order[idx];
-      const double d = pull_delta(a, dc, delta, v);
-      delta[v] = d;
+      const double d = pull_delta(a, rec, v);
+      set_delta(&rec[v], d);
       atomicAdd(a.bc + v, 0.5 * d);
     }
     __syncthreads();
@@ -655,9 +661,8 @@ __global__ void __launch_bounds__(256) k_dependency(DepArgs a) {
   if (slot >= a.ns) return;
   const int s = a.src[slot];
   const size_t base = (size_t)slot * a.n_pad;
-  const RowView<const int2> dc{a.dc, slot, a.ns};
+  const RowView<int4> rec{a.rec, slot, a.ns};
   const RowView<const int32_t> hop{a.hop, slot, a.ns};
-  double *delta = a.delta + base;
   int32_t *order = a.order + base;
 
   int mx = 0;
@@ -691,52 +696,46 @@ __global__ void __launch_bounds__(256) k_dependency(DepArgs a) {
     }
   }
   __syncthreads();
-  backprop_levels(a, dc, delta, order, cnt, maxL);
+  backprop_levels(a, rec, order, cnt, maxL);
 }
 
 // Warp-per-source form of k_dependency for graphs whose per-source DAG is narrow: no CTA-wide
 // barrier per layer (a __syncwarp orders the layer's delta writes), many sources in flight per SM
 // to cover the gathers' DRAM latency, and the largest layer taken from the label kernel.
 // delta of vertex v with its SP-DAG out-arcs gathered four at a time: the (head, weight) pairs of up
-// to four arcs are loaded together, then their heads' (dist, sigma) and delta together, so a vertex
-// costs two rounds of memory latency per four arcs instead of two per arc.  Same FP64 operation
-// order and arc order as pull_delta.
-template <class DC>
-__device__ __forceinline__ double pull_delta4(const DepArgs &a, const DC &dc, const double *delta, int v) {
-  const int2 dv = dc[v];
+// to four arcs are loaded together, then their heads' records together, so a vertex costs two
+// rounds of memory latency per four arcs instead of two per arc.  Same FP64 operation order and arc
+// order as pull_delta.
+template <class RV>
+__device__ __forceinline__ double pull_delta4(const DepArgs &a, const RV &rec, int v) {
+  const int4 rv = rec[v];
   const int2 rng = a.arc_rng[v];
-  const double sv = (double)dv.y;
+  const double sv = (double)rv.y;
   double acc = 0.0;
   for (int e = rng.x; e < rng.y; e += 4) {
     int2 hw[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) hw[q] = (e + q < rng.y) ? a.arc_hw[e + q] : make_int2(-1, 0);
-    int2 dw[4];
-    double dl[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      if (hw[q].x >= 0) {
-        dw[q] = dc[hw[q].x];
-        dl[q] = delta[hw[q].x];
-      }
-    }
+    int4 rw[4];
 #pragma unroll
     for (int q = 0; q < 4; q++)
-      if (hw[q].x >= 0 && dw[q].x == dv.x + hw[q].y) acc += sv * (1.0 + dl[q]) / (double)dw[q].y;
+      if (hw[q].x >= 0) rw[q] = rec[hw[q].x];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (hw[q].x >= 0 && rw[q].x == rv.x + hw[q].y) acc += sv * (1.0 + rec_delta(rw[q])) / (double)rw[q].y;
   }
   return acc;
 }
 
-__global__ void __launch_bounds__(256, 4) k_dependency_warp(DepArgs a, const int32_t *__restrict__ maxhop, int lcap) {
+__global__ void __launch_bounds__(256, 3) k_dependency_warp(DepArgs a, const int32_t *__restrict__ maxhop, int lcap) {
   extern __shared__ int smw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const int slot = blockIdx.x * nwarps + warp;
   if (slot >= a.ns) return;
   const int s = a.src[slot];
   const size_t base = (size_t)slot * a.n_pad;
-  const RowView<const int2> dc{a.dc, slot, a.ns};
+  const RowView<int4> rec{a.rec, slot, a.ns};
   const RowView<const int32_t> hop{a.hop, slot, a.ns};
-  double *delta = a.delta + base;
   int32_t *order = a.order + base;
   const int maxL = maxhop[slot];
   int *cnt, *cur;
@@ -808,12 +807,12 @@ __global__ void __launch_bounds__(256, 4) k_dependency_warp(DepArgs a, const int
       const bool two = idx + 32 < e;
       const int v1 = order[idx];
       const int v2 = two ? order[idx + 32] : v1;
-      const double d1 = pull_delta4(a, dc, delta, v1);
-      const double d2 = two ? pull_delta4(a, dc, delta, v2) : 0.0;
-      delta[v1] = d1;
+      const double d1 = pull_delta4(a, rec, v1);
+      const double d2 = two ? pull_delta4(a, rec, v2) : 0.0;
+      set_delta(&rec[v1], d1);
       atomicAdd(a.bc + v1, 0.5 * d1);
       if (two) {
-        delta[v2] = d2;
+        set_delta(&rec[v2], d2);
         atomicAdd(a.bc + v2, 0.5 * d2);
       }
     }
@@ -830,23 +829,22 @@ __global__ void __launch_bounds__(256) k_kahn_dependency(DepArgs a) {
   if (slot >= a.ns) return;
   const int s = a.src[slot];
   const size_t base = (size_t)slot * a.n_pad;
-  const RowView<int2> dc{a.dc, slot, a.ns};
+  const RowView<int4> rec{a.rec, slot, a.ns};
   const RowView<int32_t> deg{a.hop, slot, a.ns};
-  double *delta = a.delta + base;
   int32_t *order = a.order + base;
   int *wave = sh_wave;
   bool global_waves = false;
   int wave_cap = kLayerCap;
   // in-degree over reverse arcs (arcs are symmetric) and sigma = 0
   for (int v = threadIdx.x; v < a.n; v += blockDim.x) {
-    const int dv = dc[v].x;
+    const int dv = rec[v].x;
     int c = 0;
     for (int e = a.arc_off[v]; e < a.arc_off[v + 1]; e++) {
       const int u = a.arc_head[e];
-      if (dc[u].x + a.arc_w[e] == dv) c++;
+      if (rec[u].x + a.arc_w[e] == dv) c++;
     }
     deg[v] = c;
-    dc[v].y = (v == s) ? 1 : 0;
+    rec[v].y = (v == s) ? 1 : 0;
   }
   if (threadIdx.x == 0) {
     order[0] = s;
@@ -863,11 +861,11 @@ __global__ void __launch_bounds__(256) k_kahn_dependency(DepArgs a) {
     if (b == e) break;
     for (int idx = b + threadIdx.x; idx < e; idx += blockDim.x) {
       const int v = order[idx];
-      const int2 dv = dc[v];
+      const int4 dv = rec[v];
       for (int ee = a.arc_off[v]; ee < a.arc_off[v + 1]; ee++) {
         const int w = a.arc_head[ee];
-        if (dc[w].x == dv.x + a.arc_w[ee]) {
-          atomicAdd(&dc[w].y, dv.y);
+        if (rec[w].x == dv.x + a.arc_w[ee]) {
+          atomicAdd(&rec[w].y, dv.y);
           if (atomicSub(&deg[w], 1) == 1) {
             const int pos = atomicAdd(&s_tail, 1);
             order[pos] = w;
@@ -903,7 +901,7 @@ __global__ void __launch_bounds__(256) k_kahn_dependency(DepArgs a) {
   }
   __syncthreads();
   // waves 1..L-1 hold vertices; wave L is empty
-  backprop_levels(a, dc, delta, order, wave, L - 1);
+  backprop_levels(a, rec, order, wave, L - 1);
 }
 
 __global__ void k_tid_to_vid_f64(const double *__restrict__ in, const int32_t *__restrict__ vid_of, double *out,
@@ -924,14 +922,14 @@ __global__ void k_vid_to_tid(const int32_t *__restrict__ vids, const int32_t *__
   }
 }
 
-__global__ void k_rows_to_vid(const int2 *__restrict__ dc, const int32_t *__restrict__ hop,
+__global__ void k_rows_to_vid(const int4 *__restrict__ rec, const int32_t *__restrict__ hop,
                               const int32_t *__restrict__ vid_of, int n, int n_pad, int ns, int32_t *dist,
                               uint32_t *cnt, int32_t *hp) {
   const int slot = blockIdx.y;
   if (slot >= ns) return;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const int v = vid_of[t];
-    const int2 x = dc[blk(slot, t, ns)];
+    const int4 x = rec[blk(slot, t, ns)];
     dist[(size_t)slot * n + v] = x.x;
     if (cnt) cnt[(size_t)slot * n + v] = (uint32_t)x.y;
     if (hp) hp[(size_t)slot * n + v] = hop[blk(slot, t, ns)];
@@ -1059,7 +1057,7 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t
   a.n_pad = d->n_pad;
   a.stride = p.S;
   a.split = p.split;
-  a.out_dc = d->dc[buf];
+  a.out_rec = d->rec[buf];
   a.out_hop = d->hop[buf];
   a.maxhop = d->maxhop[buf];
   a.aend = d->aend;
@@ -1096,9 +1094,8 @@ static DepArgs dep_args(DeviceState *d, int buf, const int32_t *src, int32_t ns)
   a.ns = ns;
   a.n = d->n;
   a.n_pad = d->n_pad;
-  a.dc = d->dc[buf];
+  a.rec = d->rec[buf];
   a.hop = d->hop[buf];
-  a.delta = d->delta[buf];
   a.order = d->order[buf];
   a.lcnt = d->lcnt[buf];
   a.bc = d->bc_tid;
@@ -1154,17 +1151,16 @@ void launch_vid_to_tid(DeviceState *d, const int32_t *vids, int32_t *tids, int32
   d->launches++;
 }
 
-// Per-source scratch: two buffers of `chunk` source slots (24 B per vertex and slot plus the layer
+// Per-source scratch: one buffer of `chunk` source slots (24 B per vertex and slot plus the layer
 // counters).  `chunk` comes from the tuning, else from the free memory left after the index.
 static void free_scratch(DeviceState *d) {
   sweep_cache_free(d);
   for (int b = 0; b < 2; b++) {
-    void *q[] = {d->dc[b], d->hop[b], d->delta[b], d->order[b], d->lcnt[b], d->src[b], d->maxhop[b]};
+    void *q[] = {d->rec[b], d->hop[b], d->order[b], d->lcnt[b], d->src[b], d->maxhop[b]};
     for (void *p : q)
       if (p) cudaFree(p);
-    d->dc[b] = nullptr;
+    d->rec[b] = nullptr;
     d->hop[b] = d->order[b] = d->lcnt[b] = d->src[b] = d->maxhop[b] = nullptr;
-    d->delta[b] = nullptr;
   }
   d->bytes -= d->scratch_bytes;
   d->scratch_bytes = 0;
@@ -1174,21 +1170,21 @@ static void free_scratch(DeviceState *d) {
 static void alloc_scratch(Handle &h, DeviceState *d) {
   const Index &ix = h.host;
   const int64_t before = d->bytes;
-  const size_t per_slot = (size_t)d->n_pad * (8 + 4 + 8 + 4) + (size_t)2 * (d->n_pad + 2) * 4 + 4;
+  const size_t per_slot = (size_t)d->n_pad * (16 + 4 + 4) + (size_t)2 * (d->n_pad + 2) * 4 + 4;
   size_t free_b = 0, total_b = 0;
   CK(cudaMemGetInfo(&free_b, &total_b));
   int32_t chunk = h.tuning.chunk;
   if (chunk <= 0) {
     const size_t budget = std::min<size_t>(free_b / 4, (size_t)24 << 30);
-    chunk = (int32_t)std::max<size_t>(32, std::min<size_t>(4096, budget / (2 * per_slot)));
+    chunk = (int32_t)std::max<size_t>(32, std::min<size_t>(4096, budget / per_slot));
     chunk = std::max(32, (chunk / 32) * 32);
   }
   chunk = std::min<int32_t>(chunk, std::max(32, (ix.n + 31) / 32 * 32));
   d->chunk = chunk;
-  for (int b = 0; b < 2; b++) {
-    d->dc[b] = dmalloc<int2>(d, (size_t)chunk * d->n_pad);
+  // one buffer: the label scan and dependency pass of consecutive chunks run in order on one stream
+  for (int b = 0; b < 1; b++) {
+    d->rec[b] = dmalloc<int4>(d, (size_t)chunk * d->n_pad);
     d->hop[b] = dmalloc<int32_t>(d, (size_t)chunk * d->n_pad);
-    d->delta[b] = dmalloc<double>(d, (size_t)chunk * d->n_pad);
     d->order[b] = dmalloc<int32_t>(d, (size_t)chunk * d->n_pad);
     d->lcnt[b] = dmalloc<int32_t>(d, (size_t)chunk * 2 * (d->n_pad + 2));
     d->src[b] = dmalloc<int32_t>(d, (size_t)chunk);
@@ -1327,11 +1323,9 @@ void device_bc_sources(Handle &h, const int32_t *d_sources0, int32_t ns, double 
   CK(cudaMemsetAsync(d->bc_tid, 0, (size_t)d->n * 8, d->s_label));
   CK(cudaEventRecord(d->ev_label[1], d->s_label));
   CK(cudaStreamWaitEvent(d->s_dep, d->ev_label[1], 0));
-  int k = 0;
-  for (int32_t off = 0; off < ns; off += d->chunk, k++) {
-    const int b = k & 1;
+  for (int32_t off = 0; off < ns; off += d->chunk) {
+    const int b = 0;  // stream order frees the buffer for the next chunk
     const int32_t cnt = std::min(d->chunk, ns - off);
-    if (k >= 2) CK(cudaStreamWaitEvent(d->s_label, d->ev_dep[b], 0));  // buffer b free again
     k_vid_to_tid<<<(cnt + 255) / 256, 256, 0, d->s_label>>>(d_sources0 + off, d->tid_of, d->src[b], cnt, d->n, d->err);
     CK(cudaGetLastError());
     d->launches++;
@@ -1339,7 +1333,6 @@ void device_bc_sources(Handle &h, const int32_t *d_sources0, int32_t ns, double 
     // The dependency pass runs right after the scan on the same stream: run concurrently on a
     // second stream the two kernels thrash each other's caches and both slow down ~2x.
     launch_dep(h, d, b, d->src[b], cnt, d->s_label);
-    CK(cudaEventRecord(d->ev_dep[b], d->s_label));
   }
   CK(cudaEventRecord(d->ev_dep[0], d->s_label));
   CK(cudaStreamWaitEvent(user, d->ev_dep[0], 0));
@@ -1451,7 +1444,7 @@ void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, ui
         launch_dep(h, d, 0, d->src[0], c, st);
       }
       dim3 grid((n + 255) / 256, c);
-      k_rows_to_vid<<<grid, 256, 0, st>>>(d->dc[0], d->hop[0], d->vid_of, n, d->n_pad, c, o_d, o_c, o_h);
+      k_rows_to_vid<<<grid, 256, 0, st>>>(d->rec[0], d->hop[0], d->vid_of, n, d->n_pad, c, o_d, o_c, o_h);
       CK(cudaGetLastError());
       CK(cudaMemcpyAsync(dist + (size_t)off * n, o_d, (size_t)c * n * 4, cudaMemcpyDeviceToHost, st));
       if (cnt) CK(cudaMemcpyAsync(cnt + (size_t)off * n, o_c, (size_t)c * n * 4, cudaMemcpyDeviceToHost, st));
@@ -1479,10 +1472,9 @@ void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, ui
 // this statically sized device array instead of the index's allocated scratch buffers.  Every GPU
 // that loads the library holds it (kStaticScratchBytes, about 5 MiB) until the process exits.
 constexpr int32_t kStaticMaxVertices = 1 << 17;  // largest graph the static scratch serves
-constexpr size_t kStaticDc = 0;                                                     // int2[max]
-constexpr size_t kStaticHop = kStaticDc + (size_t)kStaticMaxVertices * 8;           // int32[max]
-constexpr size_t kStaticDelta = kStaticHop + (size_t)kStaticMaxVertices * 4;        // double[max]
-constexpr size_t kStaticOrder = kStaticDelta + (size_t)kStaticMaxVertices * 8;      // int32[max]
+constexpr size_t kStaticRec = 0;                                                    // int4[max]
+constexpr size_t kStaticHop = kStaticRec + (size_t)kStaticMaxVertices * 16;         // int32[max]
+constexpr size_t kStaticOrder = kStaticHop + (size_t)kStaticMaxVertices * 4;        // int32[max]
 constexpr size_t kStaticLcnt = kStaticOrder + (size_t)kStaticMaxVertices * 4;       // int32[2*(max+2)]
 constexpr size_t kStaticBc = kStaticLcnt + (((size_t)2 * (kStaticMaxVertices + 2) * 4 + 255) / 256) * 256;  // double[max]
 constexpr size_t kStaticSrc = kStaticBc + (size_t)kStaticMaxVertices * 8;           // int32[64]
@@ -1520,9 +1512,8 @@ void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *s
   DeviceState *d = need_dev(h);
   unsigned char *base = static_scratch_on(d->device);
   cudaStream_t st = stream ? (cudaStream_t)stream : d->s_label;
-  int2 *dc = reinterpret_cast<int2 *>(base + kStaticDc);
+  int4 *rec = reinterpret_cast<int4 *>(base + kStaticRec);
   int32_t *hop = reinterpret_cast<int32_t *>(base + kStaticHop);
-  double *delta = reinterpret_cast<double *>(base + kStaticDelta);
   int32_t *order = reinterpret_cast<int32_t *>(base + kStaticOrder);
   int32_t *lcnt = reinterpret_cast<int32_t *>(base + kStaticLcnt);
   double *bc_tid = reinterpret_cast<double *>(base + kStaticBc);
@@ -1546,7 +1537,7 @@ void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *s
   la.n_pad = d->n_pad;
   la.stride = p.S;
   la.split = p.split;
-  la.out_dc = dc;
+  la.out_rec = rec;
   la.out_hop = hop;
   if (h.host.kind == IndexKind::MHL) launch_label_c<true>(p, la, 1, st);
   else launch_label_c<false>(p, la, 1, st);
@@ -1558,9 +1549,8 @@ void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *s
   da.ns = 1;
   da.n = d->n;
   da.n_pad = d->n_pad;
-  da.dc = dc;
+  da.rec = rec;
   da.hop = hop;
-  da.delta = delta;
   da.order = order;
   da.lcnt = lcnt;
   da.bc = bc_tid;

@@ -37,11 +37,10 @@ struct DeviceState {
   int32_t packed_bits = 0;  // > 0: the packed-key label scan applies
   int64_t *lab_off = nullptr;
   int2 *ch = nullptr;
-  // scratch, two buffers of `chunk` slots
+  // scratch: one buffer of `chunk` source slots (index 1 unused)
   int32_t chunk = 0;
-  int2 *dc[2] = {nullptr, nullptr};
+  int4 *rec[2] = {nullptr, nullptr};  // per (slot, vertex): dist, sigma bits, delta (f64)
   int32_t *hop[2] = {nullptr, nullptr};
-  double *delta[2] = {nullptr, nullptr};
   int32_t *order[2] = {nullptr, nullptr};
   int32_t *lcnt[2] = {nullptr, nullptr};
   int32_t *src[2] = {nullptr, nullptr};

@@ -351,7 +351,7 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
     }
     // 4. sources per scratch buffer
     for (int32_t ch : {1024, 2048, 4096, 8192}) {
-      if (ch > std::max<int32_t>(32, (h.host.n + 31) / 32 * 32)) continue;
+      if (ch > std::max<int32_t>(32, (cnt + 31) / 32 * 32)) continue;  // the sample must span a chunk
       Tuning t = best;
       t.chunk = ch;
       trial(t);
@@ -431,7 +431,7 @@ struct Server {
   DeviceState *d = nullptr;
   cudaStream_t st = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
-  int32_t ns = 0, nchunks = 0;
+  int32_t ns = 0, nchunks = 0, chunk = 0;
   int32_t *d_tids = nullptr;
   std::vector<cudaGraphExec_t> graphs;  // one per chunk
   Counters per_chunk{0, 0, 0};
@@ -613,7 +613,12 @@ Server *serve_open(Handle &h, const int32_t *sources0, int32_t ns, const int64_t
     std::vector<int32_t> tids = source_tids(h.host, sources0, ns);
     if (tids.empty()) throw Error(QBC_EINVAL, "empty source list");
     s->ns = (int32_t)tids.size();
-    s->nchunks = (s->ns + d->chunk - 1) / d->chunk;
+    // sources per served chunk: the admission granularity (at most the scratch's chunk)
+    int32_t sc = nopts > 3 && opts[3] > 0 ? (int32_t)std::min<int64_t>(opts[3], d->chunk) : d->chunk;
+    sc = std::max<int32_t>(32, (sc + 31) / 32 * 32);
+    sc = std::min(sc, d->chunk);
+    s->chunk = sc;
+    s->nchunks = (s->ns + sc - 1) / sc;
     const int64_t max_active = nopts > 0 && opts[0] > 0 ? opts[0] : 64;
     int64_t pool_bytes = nopts > 1 ? opts[1] : 0;
     if (nopts > 2 && opts[2] > 0) s->max_queue = (size_t)opts[2];
@@ -640,7 +645,7 @@ Server *serve_open(Handle &h, const int32_t *sources0, int32_t ns, const int64_t
     CK(cudaMemsetAsync(s->d_count, 0, 4, s->st));
     CK(cudaStreamSynchronize(s->st));
     for (int32_t c = 0; c < s->nchunks; c++) {
-      const int32_t off = c * d->chunk, cnt = std::min(d->chunk, s->ns - off);
+      const int32_t off = c * s->chunk, cnt = std::min(s->chunk, s->ns - off);
       Server *sp = s.get();
       s->graphs.push_back(capture(d, s->st, s->per_chunk, [&] {
         CK(cudaMemsetAsync(d->bc_tid, 0, (size_t)d->n * 8, sp->st));

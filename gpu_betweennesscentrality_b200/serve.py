@@ -22,13 +22,14 @@ STAT_KEYS = ("chunks", "turns", "done", "active", "queued", "pool_used", "pool_c
 
 
 class Server:
-    def __init__(self, index, sources=None, max_active: int = 64, pool_bytes: int = 0, max_queue: int = 0):
+    def __init__(self, index, sources=None, max_active: int = 64, pool_bytes: int = 0, max_queue: int = 0,
+                 chunk: int = 0):
         self.index = index
         self.h = C.c_void_p()
         src = None if sources is None else i32(sources)
-        opts = np.array([max_active, pool_bytes, max_queue], np.int64)
+        opts = np.array([max_active, pool_bytes, max_queue, chunk], np.int64)
         check(lib().qbc_serve_open(index.h, None if src is None else ptr(src, i32p),
-                                   0 if src is None else int(src.shape[0]), ptr(opts, i64p), 3, C.byref(self.h)))
+                                   0 if src is None else int(src.shape[0]), ptr(opts, i64p), 4, C.byref(self.h)))
         self._sizes = {}
 
     def submit(self, points) -> int:

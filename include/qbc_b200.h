@@ -160,7 +160,8 @@ int qbc_bc_query_batch(qbc_index *idx, const int32_t *points0, const int32_t *se
  * opts[0] requests are active (default 64) and its q accumulators fit in the request pool of
  * opts[1] bytes (16 B per query vertex; 0 = min(free device memory / 8, 64 MiB)); it completes
  * after one full turn over the sources from its admission, so its values equal qbc_bc_query's
- * (up to FP64 summation order) whatever else runs.  opts[2] = queue capacity (0 = 2^20).  While a
+ * (up to FP64 summation order) whatever else runs.  opts[2] = queue capacity (0 = 2^20);
+ * opts[3] = sources per served chunk, the admission granularity (0 = the index's chunk).  While a
  * server is open the index refuses every other device call with QBC_EBUSY.
  * times (3 doubles, may be NULL) = submit, admission and completion in seconds since open. */
 typedef struct qbc_server qbc_server;

@@ -168,6 +168,17 @@ def test_serve_source_sample_and_threads(g2k):
         assert rel_err(got[k], part[s]) <= BC_RTOL
 
 
+def test_serve_own_chunk_size(g2k):
+    n, idx, full = g2k
+    sets = request_sets(n, 6, 1, 900, seed=16)
+    with idx.serve(chunk=90) as srv:  # rounded up to a multiple of 32: 96 sources per admission point
+        res = [srv.wait(srv.submit(s), 120.0)[0] for s in sets]
+        st = srv.stats()
+    assert st["chunks_per_turn"] == (n + 95) // 96
+    for s, vals in zip(sets, res):
+        assert rel_err(vals, full[s]) <= BC_RTOL
+
+
 def test_poisson_load_2k(g2k):
     n, idx, full = g2k
     idx.set_tuning(chunk=256)
