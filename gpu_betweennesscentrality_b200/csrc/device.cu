@@ -617,41 +617,27 @@ __device__ __forceinline__ int agg_inc(int *ctr, int key, unsigned act) {
   return base + rank;
 }
 
-// A vertex's per-source record is 16 bytes: (dist, sigma bits, delta as f64), so one load brings
-// everything the backprop needs about a DAG successor.  Records are read with plain (coherent)
-// loads: delta is written during the pass.
-__device__ __forceinline__ double rec_delta(const int4 r) { return __hiloint2double(r.w, r.z); }
-__device__ __forceinline__ void set_delta(int4 *r, double d) { reinterpret_cast<double *>(r)[1] = d; }
+// Dependencies (MHLQBC.cu:452-466): delta_v = sum over DAG arcs v->w of sigma_v * (1 + delta_w) /
+// sigma_w.  Factored as delta_v = sigma_v * sum_w rho_w with rho_w = (1 + delta_w) / sigma_w, one
+// FP64 division per vertex instead of one per DAG arc; this reassociation changes results only by
+// rounding (relative 1e-14 at the tested sizes; the BC tolerance is 1e-9).  A vertex's per-source
+// record is 16 bytes: (dist, sigma bits, rho as f64), so one load brings everything the backprop
+// needs about a DAG successor.  Records are read with plain (coherent) loads: rho is written
+// during the pass.
+__device__ __forceinline__ double rec_rho(const int4 r) { return __hiloint2double(r.w, r.z); }
+__device__ __forceinline__ void set_rho(int4 *r, double x) { reinterpret_cast<double *>(r)[1] = x; }
 
-// Pull-form dependency of vertex v (MHLQBC.cu:452-466): delta(v) = sum over DAG arcs v->w of
-// sigma_v * (1 + delta_w) / sigma_w, operation order as the reference (:457).
+// delta of v, its rho stored in its record, 0.5 * delta added into BC
 template <class RV>
-__device__ __forceinline__ double pull_delta(const DepArgs &a, const RV &rec, int v) {
-  const int4 rv = rec[v];
-  const double sv = (double)rv.y;
-  double acc = 0.0;
-  const int e1 = a.arc_off[v + 1];
-  for (int e = a.arc_off[v]; e < e1; e++) {
-    const int w = a.arc_head[e];
-    const int4 rw = rec[w];
-    if (rw.x == rv.x + a.arc_w[e]) acc += sv * (1.0 + rec_delta(rw)) / (double)rw.y;
-  }
-  return acc;
+__device__ __forceinline__ void finish_vertex(const DepArgs &a, const RV &rec, int v, double sv, double sum) {
+  const double d = sv * sum;
+  set_rho(&rec[v], (1.0 + d) / sv);
+  atomicAdd(a.bc + v, 0.5 * d);
 }
 
+// layered backprop over a level queue by a whole CTA (defined after the 4-wide gather below)
 template <class RV>
-__device__ void backprop_levels(const DepArgs &a, const RV &rec, const int32_t *order, const int *start, int maxL) {
-  for (int L = maxL; L >= 1; --L) {
-    const int b = start[L], e = start[L + 1];
-    for (int idx = b + threadIdx.x; idx < e; idx += blockDim.x) {
-      const int v = order[idx];
-      const double d = pull_delta(a, rec, v);
-      set_delta(&rec[v], d);
-      atomicAdd(a.bc + v, 0.5 * d);
-    }
-    __syncthreads();
-  }
-}
+__device__ void backprop_levels(const DepArgs &a, const RV &rec, const int32_t *order, const int *start, int maxL);
 
 __global__ void __launch_bounds__(256) k_dependency(DepArgs a) {
   __shared__ int sh_cnt[kLayerCap + 2];
@@ -702,15 +688,14 @@ __global__ void __launch_bounds__(256) k_dependency(DepArgs a) {
 // Warp-per-source form of k_dependency for graphs whose per-source DAG is narrow: no CTA-wide
 // barrier per layer (a __syncwarp orders the layer's delta writes), many sources in flight per SM
 // to cover the gathers' DRAM latency, and the largest layer taken from the label kernel.
-// delta of vertex v with its SP-DAG out-arcs gathered four at a time: the (head, weight) pairs of up
-// to four arcs are loaded together, then their heads' records together, so a vertex costs two
-// rounds of memory latency per four arcs instead of two per arc.  Same FP64 operation order and arc
-// order as pull_delta.
+// sum of rho over v's SP-DAG out-arcs gathered four at a time: the (head, weight) pairs of up to
+// four arcs are loaded together, then their heads' records together, so a vertex costs two rounds
+// of memory latency per four arcs instead of two per arc; arcs are summed in CSR order.
 template <class RV>
-__device__ __forceinline__ double pull_delta4(const DepArgs &a, const RV &rec, int v) {
+__device__ __forceinline__ double pull_rho_sum4(const DepArgs &a, const RV &rec, int v, double &sv) {
   const int4 rv = rec[v];
   const int2 rng = a.arc_rng[v];
-  const double sv = (double)rv.y;
+  sv = (double)rv.y;
   double acc = 0.0;
   for (int e = rng.x; e < rng.y; e += 4) {
     int2 hw[4];
@@ -722,11 +707,46 @@ __device__ __forceinline__ double pull_delta4(const DepArgs &a, const RV &rec, i
       if (hw[q].x >= 0) rw[q] = rec[hw[q].x];
 #pragma unroll
     for (int q = 0; q < 4; q++)
-      if (hw[q].x >= 0 && rw[q].x == rv.x + hw[q].y) acc += sv * (1.0 + rec_delta(rw[q])) / (double)rw[q].y;
+      if (hw[q].x >= 0 && rw[q].x == rv.x + hw[q].y) acc += rec_rho(rw[q]);
   }
   return acc;
 }
 
+template <class RV>
+__device__ void backprop_levels(const DepArgs &a, const RV &rec, const int32_t *order, const int *start, int maxL) {
+  for (int L = maxL; L >= 1; --L) {
+    const int b = start[L], e = start[L + 1];
+    for (int idx = b + threadIdx.x; idx < e; idx += blockDim.x) {
+      const int v = order[idx];
+      double sv;
+      const double sum = pull_rho_sum4(a, rec, v, sv);
+      finish_vertex(a, rec, v, sv, sum);
+    }
+    __syncthreads();
+  }
+}
+
+// One step of the pipelined backprop: up to 32 vertices of one layer, one per lane.
+struct StepIt {
+  int L, idx, end;  // layer, first queue position of the step, end of the layer
+};
+
+__device__ __forceinline__ StepIt step_first(const int *cnt, int maxL) {
+  int L = maxL;
+  while (L >= 1 && cnt[L] == cnt[L + 1]) L--;
+  return StepIt{L, L >= 1 ? cnt[L] : 0, L >= 1 ? cnt[L + 1] : 0};
+}
+
+__device__ __forceinline__ StepIt step_next(const int *cnt, StepIt it) {
+  if (it.L < 1) return it;
+  it.idx += 32;
+  if (it.idx < it.end) return it;
+  int L = it.L - 1;
+  while (L >= 1 && cnt[L] == cnt[L + 1]) L--;
+  return StepIt{L, L >= 1 ? cnt[L] : 0, L >= 1 ? cnt[L + 1] : 0};
+}
+
+template <bool PIPE>
 __global__ void __launch_bounds__(256, 3) k_dependency_warp(DepArgs a, const int32_t *__restrict__ maxhop, int lcap) {
   extern __shared__ int smw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
@@ -800,23 +820,85 @@ __global__ void __launch_bounds__(256, 3) k_dependency_warp(DepArgs a, const int
     }
   }
   __syncwarp();
-  // layers from the deepest up; two vertices per lane per step so their gathers overlap
-  for (int L = maxL; L >= 1; --L) {
-    const int b = cnt[L], e = cnt[L + 1];
-    for (int idx = b + lane; idx < e; idx += 64) {
-      const bool two = idx + 32 < e;
-      const int v1 = order[idx];
-      const int v2 = two ? order[idx + 32] : v1;
-      const double d1 = pull_delta4(a, rec, v1);
-      const double d2 = two ? pull_delta4(a, rec, v2) : 0.0;
-      set_delta(&rec[v1], d1);
-      atomicAdd(a.bc + v1, 0.5 * d1);
-      if (two) {
-        set_delta(&rec[v2], d2);
-        atomicAdd(a.bc + v2, 0.5 * d2);
+  if constexpr (PIPE) {
+    // Software-pipelined backprop: everything about a vertex that does not change during the pass
+    // (its queue entry, its dist/sigma, its arc range, its first four arcs) is loaded one to three
+    // steps ahead, so a step waits only for its successors' records (rho written by the previous
+    // layer).  Steps never cross a layer; a __syncwarp separates layers.
+    StepIt itC = step_first(cnt, maxL);  // step being computed
+    StepIt itB = step_next(cnt, itC);    // its successor: records + arc ranges arriving
+    StepIt itA = step_next(cnt, itB);    // the one after: queue entry arriving
+    auto vertex_at = [&](const StepIt &it) { return (it.L >= 1 && it.idx + lane < it.end) ? order[it.idx + lane] : -1; };
+    // stage C (compute) registers
+    int vC = vertex_at(itC);
+    int4 rC = vC >= 0 ? rec[vC] : make_int4(0, 0, 0, 0);
+    int2 gC = vC >= 0 ? a.arc_rng[vC] : make_int2(0, 0);
+    int2 hC[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) hC[q] = (gC.x + q < gC.y) ? a.arc_hw[gC.x + q] : make_int2(-1, 0);
+    // stage B registers
+    int vB = vertex_at(itB);
+    int4 rB = vB >= 0 ? rec[vB] : make_int4(0, 0, 0, 0);
+    int2 gB = vB >= 0 ? a.arc_rng[vB] : make_int2(0, 0);
+    // stage A register
+    int vA = vertex_at(itA);
+    while (itC.L >= 1) {
+      // issue the look-ahead loads first
+      int2 hB[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) hB[q] = (gB.x + q < gB.y) ? a.arc_hw[gB.x + q] : make_int2(-1, 0);
+      const int4 rA = vA >= 0 ? rec[vA] : make_int4(0, 0, 0, 0);
+      const int2 gA = vA >= 0 ? a.arc_rng[vA] : make_int2(0, 0);
+      const StepIt itN = step_next(cnt, itA);
+      const int vN = vertex_at(itN);
+      // compute step C: its successors' records (rho written by earlier layers)
+      if (vC >= 0) {
+        int4 rw[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (hC[q].x >= 0) rw[q] = rec[hC[q].x];
+        double acc = 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (hC[q].x >= 0 && rw[q].x == rC.x + hC[q].y) acc += rec_rho(rw[q]);
+        for (int e = gC.x + 4; e < gC.y; e++) {  // arcs beyond the first four, in arc order
+          const int2 hw = a.arc_hw[e];
+          const int4 r = rec[hw.x];
+          if (r.x == rC.x + hw.y) acc += rec_rho(r);
+        }
+        finish_vertex(a, rec, vC, (double)rC.y, acc);
       }
+      // rotate; a layer change needs this layer's rho visible to the whole warp
+      if (itB.L != itC.L) __syncwarp();
+      itC = itB;
+      vC = vB;
+      rC = rB;
+      gC = gB;
+#pragma unroll
+      for (int q = 0; q < 4; q++) hC[q] = hB[q];
+      itB = itA;
+      vB = vA;
+      rB = rA;
+      gB = gA;
+      itA = itN;
+      vA = vN;
     }
-    __syncwarp();
+  } else {
+    // layers from the deepest up; two vertices per lane per step so their gathers overlap
+    for (int L = maxL; L >= 1; --L) {
+      const int b = cnt[L], e = cnt[L + 1];
+      for (int idx = b + lane; idx < e; idx += 64) {
+        const bool two = idx + 32 < e;
+        const int v1 = order[idx];
+        const int v2 = two ? order[idx + 32] : v1;
+        double sv1, sv2 = 1.0;
+        const double r1 = pull_rho_sum4(a, rec, v1, sv1);
+        const double r2 = two ? pull_rho_sum4(a, rec, v2, sv2) : 0.0;
+        finish_vertex(a, rec, v1, sv1, r1);
+        if (two) finish_vertex(a, rec, v2, sv2, r2);
+      }
+      __syncwarp();
+    }
   }
 }
 
@@ -1119,9 +1201,14 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *
     constexpr int wpb = 8;
     const int lcap = h.tuning.queue_depth > 0 ? std::min(2048, std::max(64, h.tuning.queue_depth)) : 512;
     const size_t smem = (size_t)wpb * 2 * lcap * 4;
-    if (smem > 48 * 1024)
-      CK(cudaFuncSetAttribute(k_dependency_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_dependency_warp<<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
+    if (smem > 48 * 1024) {
+      CK(cudaFuncSetAttribute(k_dependency_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      CK(cudaFuncSetAttribute(k_dependency_warp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    // auto (0) = the software-pipelined backprop: measured fastest at 50k (162 vs 176-191 ms)
+    if (h.tuning.dep_form == 3 || h.tuning.dep_form == 0)
+      k_dependency_warp<true><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
+    else k_dependency_warp<false><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
   } else if (h.host.kind == IndexKind::MHL) {
     k_dependency<<<ns, threads, 0, st>>>(a);
   } else {
@@ -1542,6 +1629,8 @@ void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *s
   if (h.host.kind == IndexKind::MHL) launch_label_c<true>(p, la, 1, st);
   else launch_label_c<false>(p, la, 1, st);
   DepArgs da{};
+  da.arc_rng = d->arc_rng;
+  da.arc_hw = d->arc_hw;
   da.arc_off = d->arc_off;
   da.arc_head = d->arc_head;
   da.arc_w = d->arc_w;

@@ -337,12 +337,13 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
       trial(t);
     }
     // 3. dependency pass: warp per source with its shared level-queue depth, or CTA per source
-    for (int32_t qd : {256, 512, 1024}) {
-      Tuning t = best;
-      t.dep_form = 1;
-      t.queue_depth = qd;
-      trial(t);
-    }
+    for (int32_t form : {1, 3})
+      for (int32_t qd : {64, 256, 512, 1024}) {
+        Tuning t = best;
+        t.dep_form = form;
+        t.queue_depth = qd;
+        trial(t);
+      }
     for (int32_t th : {128, 256}) {
       Tuning t = best;
       t.dep_form = 2;

@@ -93,7 +93,7 @@ def test_plain_path_matches_batched(g2k):
     assert rel_err(idx.bc_sources(srcs), tc.bc(arcs, srcs)) <= BC_RTOL
 
 
-@pytest.mark.parametrize("form", [1, 2])
+@pytest.mark.parametrize("form", [1, 2, 3])
 def test_dependency_forms_agree(g2k, form):
     n, u, v, w, g, idx, tc, arcs = g2k
     srcs = np.arange(0, n, 5, dtype=np.int32)
@@ -180,7 +180,13 @@ def test_shortcut_graph_rows_and_bc():
     for k, s in enumerate(srcs):
         d0, c0, h0 = tc.rows(int(s))
         assert np.array_equal(d[k], d0) and np.array_equal(c[k], c0) and np.array_equal(h[k], h0)
-    assert rel_err(idx.bc_sources(srcs), tc.bc(O.Arcs(n, u, v, w), srcs)) <= BC_RTOL
+    want = tc.bc(O.Arcs(n, u, v, w), srcs)
+    try:
+        for form in (0, 1, 2, 3):  # shortcut vertices have more than four arcs
+            idx.set_tuning(dep_form=form, queue_depth=64 if form == 3 else 0)
+            assert rel_err(idx.bc_sources(srcs), want) <= BC_RTOL, form
+    finally:
+        idx.set_tuning()
 
 
 def test_50k_sampled_rows_and_partial_bc(graph_cache):
