@@ -227,6 +227,7 @@ def main():
     ap.add_argument("--sample", type=int, default=0,
                     help="sources per step: a seeded sample of this many vertices (0: all n, the full BC)")
     ap.add_argument("--shortcuts", type=float, default=0.0, help="fraction of n random shortcut edges (500..5000)")
+    ap.add_argument("--host-build", action="store_true", help="fill the label rows on the host (default: on the GPU)")
     ap.add_argument("--tune", action="append", default=[], metavar="KEY=VALUE",
                     help="set a tuning field (Index.TUNING_KEYS) instead of autotuning it; repeatable")
     ap.add_argument("--no-rq", action="store_true", help="skip the batched and served RQ measurements")
@@ -263,15 +264,20 @@ def main():
     G.ReadGraph(path)
     t_read = time.perf_counter() - t
     t = time.perf_counter()
-    idx = G.build_index(upload=False)
+    if args.host_build:
+        idx = G.build_index(upload=False)
+    else:  # elimination and tree on the host, label rows filled on the GPU
+        idx = G.build_index(on_device=True)
+        torch.cuda.synchronize()
     t_build = time.perf_counter() - t
     if args.chunk or args.tune:
         fixed = {"chunk": args.chunk}
         fixed.update({k: int(v) for k, v in (t.split("=", 1) for t in args.tune)})
         idx.set_tuning(**fixed)
     t = time.perf_counter()
-    idx.upload(local)
-    torch.cuda.synchronize()
+    if args.host_build:
+        idx.upload(local)
+        torch.cuda.synchronize()
     t_upload = time.perf_counter() - t
     info = idx.info()
     n = G.nodenum
@@ -400,7 +406,8 @@ def main():
                "config": _config(n, int(info[1]) // 2, n_sources, args,
                                  {"index": {"tree_height": int(info[3]), "tree_width": int(info[4]),
                                             "label_entries": int(info[7]), "device_bytes": int(info[5]),
-                                            "host_build_s": round(t_build, 3), "read_s": round(t_read, 3),
+                                            "build": "host" if args.host_build else "device rows",
+                                            "build_s": round(t_build, 3), "read_s": round(t_read, 3),
                                             "upload_s": round(t_upload, 3)},
                                   "tuning": idx.get_tuning(), "autotune": tune}),
                "e2e": {"value": e2e_val, "unit": "sources/s", "h2d_bytes_per_step": int(4 * ns),

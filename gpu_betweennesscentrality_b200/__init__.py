@@ -72,19 +72,27 @@ def read_query(path: str, n: int) -> np.ndarray:
 
 
 class Index:
-    """Tree-decomposition index of a graph, built on the host and uploaded to one GPU."""
+    """Tree-decomposition index of a graph, resident on one GPU.  ``on_device`` fills the label
+    rows on the GPU (``qbc_index_build_device``); otherwise they are built on the host and uploaded
+    to ``device`` (None: host only)."""
 
     def __init__(self, graph: _GraphHandle, kind: int = QBC_INDEX_MHL, node_order=None, nthreads: int = 0,
-                 device: Optional[int] = 0):
+                 device: Optional[int] = 0, on_device: bool = False):
         self._graph = graph
         h = C.c_void_p()
         o = None if node_order is None else i32(node_order)
-        check(lib().qbc_index_build(graph.h, int(kind), None if o is None else ptr(o, i32p), int(nthreads), C.byref(h)))
+        optr = None if o is None else ptr(o, i32p)
+        if on_device:
+            if device is None:
+                raise QbcError(1, "a device build needs a device")
+            check(lib().qbc_index_build_device(graph.h, int(kind), optr, int(device), C.byref(h)))
+        else:
+            check(lib().qbc_index_build(graph.h, int(kind), optr, int(nthreads), C.byref(h)))
         self.h = h
         info = self.info()
         self.n = int(info[0])
         self.kind = kind
-        if device is not None:
+        if device is not None and not on_device:
             self.upload(device)
 
     def __del__(self):
@@ -256,11 +264,13 @@ class Graph:
         check(lib().qbc_min_degree_order(self._g.h, ptr(o, i32p)))
         return o
 
-    def build_index(self, kind=QBC_INDEX_MHL, node_order=None, upload: bool = True) -> Index:
-        """Builds the index on the host; uploads it to ``self.device`` unless ``upload`` is False."""
+    def build_index(self, kind=QBC_INDEX_MHL, node_order=None, upload: bool = True, on_device: bool = False) -> Index:
+        """Builds the index on the host and uploads it to ``self.device`` unless ``upload`` is False;
+        with ``on_device`` the label rows are filled on ``self.device`` instead."""
         if self._g is None:
             raise QbcError(1, "ReadGraph first")
-        self.index = Index(self._g, kind, node_order, self.nthreads, self.device if upload else None)
+        self.index = Index(self._g, kind, node_order, self.nthreads, self.device if (upload or on_device) else None,
+                           on_device=on_device)
         return self.index
 
     def brandesBCIndexGPU_5(self, roadName: str, orderFile: Optional[str] = None) -> None:

@@ -37,6 +37,7 @@ SIGNATURES = {
     "qbc_min_degree_order": (C.c_int, [vp, i32p]),
     "qbc_index_build": (C.c_int, [vp, C.c_int, i32p, C.c_int, C.POINTER(vp)]),
     "qbc_index_upload": (C.c_int, [vp, C.c_int]),
+    "qbc_index_build_device": (C.c_int, [vp, C.c_int, i32p, C.c_int, C.POINTER(vp)]),
     "qbc_index_release_device": (C.c_int, [vp]),
     "qbc_index_info": (C.c_int, [vp, i64p]),
     "qbc_index_scan_entries": (C.c_int, [vp, i32p, C.c_int32, i64p]),

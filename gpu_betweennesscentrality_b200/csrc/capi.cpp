@@ -139,6 +139,22 @@ int qbc_index_build(const qbc_graph *g, int kind, const int32_t *node_order, int
   });
 }
 
+int qbc_index_build_device(const qbc_graph *g, int kind, const int32_t *node_order, int device, qbc_index **out) {
+  return guarded([&] {
+    need(g && out, "null argument");
+    need(kind == QBC_INDEX_MHL || kind == QBC_INDEX_H2H, "unknown index kind");
+    need(kind == QBC_INDEX_MHL || node_order != nullptr, "H2H index needs a node order");
+    auto p = std::make_unique<qbc_index>();
+    qbc::Separators seps;
+    std::vector<int32_t> o;
+    if (node_order) o.assign(node_order, node_order + g->g.n);
+    p->h.host = qbc::prepare_index(g->g, kind == QBC_INDEX_MHL ? qbc::IndexKind::MHL : qbc::IndexKind::H2H,
+                                   node_order ? &o : nullptr, seps);
+    qbc::device_build(p->h, device, seps);
+    *out = p.release();
+  });
+}
+
 int qbc_index_upload(qbc_index *idx, int device) {
   return guarded([&] {
     need(idx, "null index");
@@ -151,6 +167,7 @@ int qbc_index_release_device(qbc_index *idx) {
   return guarded([&] {
     need(idx, "null index");
     not_serving(idx);
+    qbc::device_download_rows(idx->h);  // device-built rows move to the host first
     qbc::device_release(idx->h);
   });
 }
@@ -185,6 +202,10 @@ int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int3
                      int32_t *dis, int32_t *ch, int32_t *anc) {
   return guarded([&] {
     need(idx, "null index");
+    if (!idx->h.host.rows_on_host) {
+      not_serving(idx);
+      qbc::device_download_rows(const_cast<qbc_index *>(idx)->h);
+    }
     const qbc::Index &ix = idx->h.host;
     auto cp = [](void *dst, const void *src, size_t bytes) {
       if (dst && bytes) std::memcpy(dst, src, bytes);

@@ -35,6 +35,7 @@
 
 namespace qbc {
 
+constexpr int kInfDist = 999999999;  // unreached label entry (TreeDecomp INF, TreeDecomp.h:58)
 constexpr int kLayerCap = 4094;  // shared-memory layer counters; deeper DAGs use global memory
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -1288,69 +1289,268 @@ void device_set_chunk(Handle &h, int32_t chunk) {
   alloc_scratch(h, d);
 }
 
+// ------------------------------------------------------------------------------- device row fill
+// Label rows built on the device (TreeDecomp.cpp:388-450 semantics, as the host builders): node p's
+// row only reads rows of its separator vertices and ancestors, which sit at smaller depth, so the
+// rows of one depth are independent -- one launch per depth, one warp per node, lanes over the
+// row's entries (coalesced reads of the separators' rows).
+struct FillArgs {
+  const int32_t *__restrict__ depth;
+  const int32_t *__restrict__ parent;
+  const int32_t *__restrict__ send;
+  const int64_t *__restrict__ lab_off;
+  const int64_t *__restrict__ sep_off;
+  const int4 *__restrict__ sep;  // (tid of x, shortcut length, count bits, max hop)
+  int32_t *dis;
+  int2 *ch;
+  int32_t *anc, *aend;
+};
+
+template <bool MHL>
+__global__ void __launch_bounds__(256) k_fill_level(FillArgs f, const int32_t *__restrict__ nodes, int count) {
+  const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (w >= count) return;
+  const int p = nodes[w];
+  const int h = f.depth[p];
+  const int64_t off = f.lab_off[p];
+  const int par = f.parent[p];
+  const int64_t poff = par >= 0 ? f.lab_off[par] : 0;
+  // ancestor row: the parent's row plus p itself
+  for (int j = lane; j < h; j += 32) {
+    const int a = (j < h - 1) ? f.anc[poff + j] : p;
+    f.anc[off + j] = a;
+    f.aend[off + j] = f.send[a];
+  }
+  __syncwarp();
+  const int64_t sb = f.sep_off[p], se = f.sep_off[p + 1];
+  for (int j = lane; j < h - 1; j += 32) {
+    int best = kInfDist;
+    unsigned c = 0;
+    int hp = 0;
+    const int64_t ajoff = MHL ? 0 : f.lab_off[f.anc[off + j]];
+    for (int64_t i = sb; i < se; i++) {
+      const int4 x = f.sep[i];
+      const int k = f.depth[x.x] - 1;
+      int nd;
+      unsigned nc = 0;
+      int nh = 0;
+      if (j <= k) {  // ancestor j is x or above x: x's own row
+        const int64_t xo = f.lab_off[x.x] + j;
+        nd = x.y + f.dis[xo];
+        if (MHL) {
+          const int2 cx = f.ch[xo];
+          nc = (unsigned)x.z * (unsigned)cx.x;
+          nh = x.w + cx.y;
+        }
+      } else if (!MHL) {  // H2H true distances: ancestor j lies below x, its row holds x
+        nd = x.y + f.dis[ajoff + k];
+      } else {
+        continue;
+      }
+      if (nd < best) {
+        best = nd;
+        c = nc;
+        hp = nh;
+      } else if (MHL && nd == best) {
+        c += nc;
+        hp = max(hp, nh);
+      }
+    }
+    f.dis[off + j] = best;
+    if (MHL) f.ch[off + j] = make_int2((int)c, hp);
+  }
+  if (lane == 0) {
+    f.dis[off + h - 1] = 0;
+    if (MHL) f.ch[off + h - 1] = make_int2(1, 0);
+  }
+}
+
+__global__ void k_max_i32(const int32_t *__restrict__ x, int64_t n, int32_t *out) {
+  int m = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) m = max(m, x[i]);
+  m = __reduce_max_sync(kFull, m);
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
 // ------------------------------------------------------------------------------- upload
-void device_upload(Handle &h, int device) {
+static DeviceState *new_state(Handle &h, int device) {
   device_release(h);
   const Index &ix = h.host;
   CK(cudaSetDevice(device));
   DeviceState *d = new DeviceState();
   h.dev = d;
   d->device = device;
+  CK(cudaStreamCreateWithFlags(&d->s_label, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&d->s_dep, cudaStreamNonBlocking));
+  for (int b = 0; b < 2; b++) {
+    CK(cudaEventCreateWithFlags(&d->ev_label[b], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&d->ev_dep[b], cudaEventDisableTiming));
+  }
+  CK(cudaEventCreateWithFlags(&d->ev_start, cudaEventDisableTiming));
+  CK(cudaDeviceGetAttribute(&d->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  d->n = ix.n;
+  d->n_pad = (ix.n + 7) & ~7;
+  int S = (ix.tree_height + 3) & ~3;
+  if (((S / 4) & 1) == 0) S += 4;  // odd number of 16-byte groups: conflict-free LDS.128 across rows
+  d->hmax_pad = S;
+  cudaStream_t st = d->s_label;
+  d->depth = dupload(d, ix.depth, st);
+  d->send = dupload(d, ix.send, st);
+  d->arc_off = dupload(d, ix.arc_off, st);
+  d->arc_head = dupload(d, ix.arc_head, st);
+  d->arc_w = dupload(d, ix.arc_w, st);
+  {
+    std::vector<int2> rng((size_t)ix.n), hw(ix.arc_head.size());
+    for (int32_t v = 0; v < ix.n; v++) rng[v] = make_int2(ix.arc_off[v], ix.arc_off[v + 1]);
+    for (size_t e = 0; e < hw.size(); e++) hw[e] = make_int2(ix.arc_head[e], ix.arc_w[e]);
+    d->arc_rng = dupload(d, rng, st);
+    d->arc_hw = dupload(d, hw, st);
+    CK(cudaStreamSynchronize(st));  // the staging vectors die here
+  }
+  d->vid_of = dupload(d, ix.vid_of, st);
+  d->tid_of = dupload(d, ix.tid_of, st);
+  d->lab_off = dupload(d, ix.lab_off, st);
+  return d;
+}
+
+static void finish_state(Handle &h, DeviceState *d) {
+  const Index &ix = h.host;
+  cudaStream_t st = d->s_label;
+  {
+    // packed keys (dist << B) | j need every row index below 2^B and 2*max_label + 1 < 2^(32-B)
+    int B = 1;
+    while ((1 << B) < ix.tree_height) B++;
+    const uint64_t room = (uint64_t)1 << (32 - B);
+    d->packed_bits = (B <= 16 && 2ull * (uint64_t)std::max(ix.max_label, 0) + 2 < room) ? B : 0;
+  }
+  alloc_scratch(h, d);
+  d->bc_tid = dmalloc<double>(d, ix.n);
+  d->bc_vid = dmalloc<double>(d, ix.n);
+  d->err = dmalloc<int32_t>(d, 1);
+  CK(cudaMemsetAsync(d->err, 0, 4, st));
+  CK(cudaStreamSynchronize(st));
+}
+
+void device_upload(Handle &h, int device) {
+  if (!h.host.rows_on_host) {
+    if (!h.dev) throw Error(QBC_EINVAL, "index rows exist only on a released device");
+    device_download_rows(h);
+  }
+  const Index &ix = h.host;
+  DeviceState *d = nullptr;
   try {
-    CK(cudaStreamCreateWithFlags(&d->s_label, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&d->s_dep, cudaStreamNonBlocking));
-    for (int b = 0; b < 2; b++) {
-      CK(cudaEventCreateWithFlags(&d->ev_label[b], cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&d->ev_dep[b], cudaEventDisableTiming));
-    }
-    CK(cudaEventCreateWithFlags(&d->ev_start, cudaEventDisableTiming));
-    CK(cudaDeviceGetAttribute(&d->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
-    d->n = ix.n;
-    d->n_pad = (ix.n + 7) & ~7;
-    int S = (ix.tree_height + 3) & ~3;
-    if (((S / 4) & 1) == 0) S += 4;  // odd number of 16-byte groups: conflict-free LDS.128 across rows
-    d->hmax_pad = S;
+    d = new_state(h, device);
     cudaStream_t st = d->s_label;
-    d->depth = dupload(d, ix.depth, st);
-    d->send = dupload(d, ix.send, st);
-    d->arc_off = dupload(d, ix.arc_off, st);
-    d->arc_head = dupload(d, ix.arc_head, st);
-    d->arc_w = dupload(d, ix.arc_w, st);
-    {
-      std::vector<int2> rng((size_t)ix.n), hw(ix.arc_head.size());
-      for (int32_t v = 0; v < ix.n; v++) rng[v] = make_int2(ix.arc_off[v], ix.arc_off[v + 1]);
-      for (size_t e = 0; e < hw.size(); e++) hw[e] = make_int2(ix.arc_head[e], ix.arc_w[e]);
-      d->arc_rng = dupload(d, rng, st);
-      d->arc_hw = dupload(d, hw, st);
-      CK(cudaStreamSynchronize(st));  // the staging vectors die here
-    }
-    d->vid_of = dupload(d, ix.vid_of, st);
-    d->tid_of = dupload(d, ix.tid_of, st);
-    d->lab_off = dupload(d, ix.lab_off, st);
     d->dis = dupload(d, ix.dis, st);
     d->anc = dupload(d, ix.anc, st);
     d->aend = dupload(d, ix.aend, st);
-    {
-      // packed keys (dist << B) | j need every row index below 2^B and 2*max_label + 1 < 2^(32-B)
-      int B = 1;
-      while ((1 << B) < ix.tree_height) B++;
-      const uint64_t room = (uint64_t)1 << (32 - B);
-      d->packed_bits = (B <= 16 && 2ull * (uint64_t)std::max(ix.max_label, 0) + 2 < room) ? B : 0;
-    }
     if (ix.kind == IndexKind::MHL) {
       d->ch = dmalloc<int2>(d, ix.ch.size() / 2);
       CK(cudaMemcpyAsync(d->ch, ix.ch.data(), ix.ch.size() * 4, cudaMemcpyHostToDevice, st));
     }
-    alloc_scratch(h, d);
-    d->bc_tid = dmalloc<double>(d, ix.n);
-    d->bc_vid = dmalloc<double>(d, ix.n);
-    d->err = dmalloc<int32_t>(d, 1);
-    CK(cudaMemsetAsync(d->err, 0, 4, st));
-    CK(cudaStreamSynchronize(st));
+    finish_state(h, d);
   } catch (...) {
     device_release(h);
     throw;
   }
+}
+
+void device_build(Handle &h, int device, const Separators &seps) {
+  Index &ix = h.host;
+  try {
+    DeviceState *d = new_state(h, device);
+    cudaStream_t st = d->s_label;
+    const int64_t L = ix.lab_off[ix.n];
+    d->dis = dmalloc<int32_t>(d, (size_t)L);
+    d->anc = dmalloc<int32_t>(d, (size_t)L);
+    d->aend = dmalloc<int32_t>(d, (size_t)L);
+    CK(cudaMemsetAsync(d->dis, 0, (size_t)L * 4, st));
+    CK(cudaMemsetAsync(d->anc, 0, (size_t)L * 4, st));
+    CK(cudaMemsetAsync(d->aend, 0, (size_t)L * 4, st));
+    const bool mhl = ix.kind == IndexKind::MHL;
+    if (mhl) {
+      d->ch = dmalloc<int2>(d, (size_t)L);
+      CK(cudaMemsetAsync(d->ch, 0, (size_t)L * 8, st));
+    }
+    // nodes grouped by depth (counting sort; preorder keeps each level in increasing tid order)
+    std::vector<int64_t> lvl((size_t)ix.tree_height + 2, 0);
+    for (int32_t t = 0; t < ix.n; t++) lvl[ix.depth[t] + 1]++;
+    for (size_t k = 1; k < lvl.size(); k++) lvl[k] += lvl[k - 1];
+    std::vector<int32_t> nodes((size_t)ix.n);
+    {
+      std::vector<int64_t> fillp(lvl.begin(), lvl.end() - 1);
+      for (int32_t t = 0; t < ix.n; t++) nodes[fillp[ix.depth[t]]++] = t;
+    }
+    // temporaries of the fill, freed at the end
+    int32_t *d_nodes = nullptr, *d_parent = nullptr, *d_max = nullptr;
+    int64_t *d_soff = nullptr;
+    int4 *d_sep = nullptr;
+    auto free_tmp = [&] {
+      void *q[] = {d_nodes, d_parent, d_max, d_soff, d_sep};
+      for (void *p : q)
+        if (p) cudaFree(p);
+    };
+    try {
+      CK(cudaMalloc(&d_nodes, nodes.size() * 4));
+      CK(cudaMalloc(&d_parent, ix.parent.size() * 4));
+      CK(cudaMalloc(&d_soff, seps.off.size() * 8));
+      CK(cudaMalloc(&d_sep, std::max<size_t>(16, seps.ent.size() * 4)));
+      CK(cudaMalloc(&d_max, 4));
+      CK(cudaMemcpyAsync(d_nodes, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(d_parent, ix.parent.data(), ix.parent.size() * 4, cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(d_soff, seps.off.data(), seps.off.size() * 8, cudaMemcpyHostToDevice, st));
+      if (!seps.ent.empty()) CK(cudaMemcpyAsync(d_sep, seps.ent.data(), seps.ent.size() * 4, cudaMemcpyHostToDevice, st));
+      CK(cudaMemsetAsync(d_max, 0, 4, st));
+      FillArgs f{d->depth, d_parent, d->send, d->lab_off, d_soff, d_sep, d->dis, d->ch, d->anc, d->aend};
+      for (int32_t k = 1; k <= ix.tree_height; k++) {
+        const int count = (int)(lvl[k + 1] - lvl[k]);
+        if (count == 0) continue;
+        const int blocks = (count + 7) / 8;
+        if (mhl) k_fill_level<true><<<blocks, 256, 0, st>>>(f, d_nodes + lvl[k], count);
+        else k_fill_level<false><<<blocks, 256, 0, st>>>(f, d_nodes + lvl[k], count);
+        CK(cudaGetLastError());
+      }
+      k_max_i32<<<148 * 4, 256, 0, st>>>(d->dis, L, d_max);
+      CK(cudaGetLastError());
+      int32_t mx = 0;
+      CK(cudaMemcpyAsync(&mx, d_max, 4, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      ix.max_label = mx;
+    } catch (...) {
+      free_tmp();
+      throw;
+    }
+    free_tmp();
+    ix.rows_on_host = false;
+    ix.dis.clear();
+    ix.ch.clear();
+    ix.anc.clear();
+    ix.aend.clear();
+    finish_state(h, d);
+  } catch (...) {
+    device_release(h);
+    throw;
+  }
+}
+
+void device_download_rows(Handle &h) {
+  Index &ix = h.host;
+  if (ix.rows_on_host) return;
+  DeviceState *d = h.dev;
+  if (!d) throw Error(QBC_EINVAL, "index rows exist only on a released device");
+  CK(cudaSetDevice(d->device));
+  const size_t L = (size_t)ix.lab_off[ix.n];
+  ix.dis.resize(L);
+  ix.anc.resize(L);
+  ix.aend.resize(L);
+  CK(cudaMemcpy(ix.dis.data(), d->dis, L * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ix.anc.data(), d->anc, L * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ix.aend.data(), d->aend, L * 4, cudaMemcpyDeviceToHost));
+  if (ix.kind == IndexKind::MHL) {
+    ix.ch.resize(2 * L);
+    CK(cudaMemcpy(ix.ch.data(), d->ch, L * 8, cudaMemcpyDeviceToHost));
+  }
+  ix.rows_on_host = true;
 }
 
 void device_release(Handle &h) {

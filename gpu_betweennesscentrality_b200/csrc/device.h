@@ -32,6 +32,10 @@ struct Handle {
 };
 
 void device_upload(Handle &h, int device);
+// Uploads the index structure and fills its label rows on the device (host rows stay empty).
+void device_build(Handle &h, int device, const Separators &seps);
+// Copies device-built label rows to the host index (no-op when they are there already).
+void device_download_rows(Handle &h);
 void device_release(Handle &h);
 // Reallocates the per-source scratch for `chunk` source slots (0 = sized from free memory).
 void device_set_chunk(Handle &h, int32_t chunk);

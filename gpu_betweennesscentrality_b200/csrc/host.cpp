@@ -307,7 +307,7 @@ Elimination eliminate(const Graph &g, const std::vector<int32_t> *fixed_order) {
 
 // Tree from an elimination: parent(x) = the separator vertex eliminated first.  Renumbers
 // vertices in DFS preorder and fills depth / parent / subtree end.
-void make_tree(const Graph &g, const Elimination &el, Index &ix) {
+void make_tree(const Graph &g, const Elimination &el, Index &ix, bool host_rows = true) {
   const int32_t n = g.n;
   std::vector<int32_t> par((size_t)n, -1);
   int32_t roots = 0, root = -1;
@@ -379,6 +379,7 @@ void make_tree(const Graph &g, const Elimination &el, Index &ix) {
     ix.depth_sum += ix.depth[t];
   }
   ix.lab_off[n] = o;
+  if (host_rows) {
   // ancestor rows: a row is its parent's row plus the node itself (preorder: parent first)
   ix.anc.assign((size_t)o, 0);
   for (int32_t t = 0; t < n; t++) {
@@ -394,6 +395,7 @@ void make_tree(const Graph &g, const Elimination &el, Index &ix) {
   for (int32_t t = 0; t < n; t++) {
     const int64_t b = ix.lab_off[t];
     for (int32_t j = 0; j < ix.depth[t]; j++) ix.aend[b + j] = ix.send[ix.anc[b + j]];
+  }
   }
   // arcs in tid space
   ix.arc_off.assign((size_t)n + 1, 0);
@@ -428,6 +430,41 @@ void fill_rows(const Index &ix, int nthreads, F &&f) {
   });
 }
 }  // namespace
+
+// Elimination (min-degree for MHL, the order file's for H2H) and tree, without label rows; the
+// separator list of each tree node goes to `seps` in tid space for the device row fill.
+Index prepare_index(const Graph &g, IndexKind kind, const std::vector<int32_t> *node_order, Separators &seps) {
+  if (kind == IndexKind::H2H) {
+    if (!node_order || (int32_t)node_order->size() != g.n) throw Error(QBC_EINVAL, "order has wrong length");
+    std::vector<char> seen((size_t)g.n, 0);
+    for (int32_t v = 0; v < g.n; v++) {
+      int32_t o = (*node_order)[v];
+      if (o < 0 || o >= g.n || seen[o]) throw Error(QBC_EINVAL, "order is not a permutation of 0..n-1");
+      seen[o] = 1;
+    }
+  }
+  Elimination el = eliminate(g, kind == IndexKind::H2H ? node_order : nullptr);
+  Index ix;
+  ix.kind = kind;
+  make_tree(g, el, ix, false);
+  const int32_t n = g.n;
+  std::vector<int64_t> xs((size_t)n, 0);
+  for (int32_t s = 0; s < n; s++) xs[ix.tid_of[el.order[s]]] = s;
+  seps.off.assign((size_t)n + 1, 0);
+  for (int32_t t = 0; t < n; t++) seps.off[t + 1] = seps.off[t] + (el.x_off[xs[t] + 1] - el.x_off[xs[t]]);
+  seps.ent.assign((size_t)seps.off[n] * 4, 0);
+  for (int32_t t = 0; t < n; t++) {
+    int64_t o = seps.off[t] * 4;
+    for (int64_t i = el.x_off[xs[t]]; i < el.x_off[xs[t] + 1]; i++) {
+      const Adj &a = el.x[i];
+      seps.ent[o++] = ix.tid_of[a.v];
+      seps.ent[o++] = a.len;
+      seps.ent[o++] = (int32_t)a.cnt;
+      seps.ent[o++] = a.hop;
+    }
+  }
+  return ix;
+}
 
 Index build_mhl(const Graph &g, int nthreads) {
   Elimination el = eliminate(g, nullptr);

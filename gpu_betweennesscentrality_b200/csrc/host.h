@@ -55,7 +55,18 @@ struct Index {
   // arcs in tid space, each tail's arcs in file order
   std::vector<int32_t> arc_off, arc_head, arc_w;
   int64_t depth_sum = 0;
+  bool rows_on_host = true;  // false: label rows (dis/ch/anc/aend) exist only on the device
 };
+
+// Separator lists in tid space, for the device row fill: node t's entries are
+// ent[4*off[t] .. 4*off[t+1]), each (tid of x, shortcut length, path count bits, max hop), in
+// elimination order of the separator.
+struct Separators {
+  std::vector<int64_t> off;
+  std::vector<int32_t> ent;
+};
+// Elimination and tree only (no label rows: dis/ch/anc/aend stay empty); max_label is unknown (0).
+Index prepare_index(const Graph &g, IndexKind kind, const std::vector<int32_t> *node_order, Separators &seps);
 
 // TreeCount-equivalent index (distance + count + max hop) by min-degree elimination.
 Index build_mhl(const Graph &g, int nthreads);

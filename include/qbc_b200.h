@@ -71,6 +71,12 @@ int qbc_min_degree_order(const qbc_graph *g, int32_t *node_order);
 int qbc_index_build(const qbc_graph *g, int kind, const int32_t *node_order, int nthreads, qbc_index **out);
 /* copies the index to HBM of `device` (cudaSetDevice semantics, QBC.cu:601-602) */
 int qbc_index_upload(qbc_index *idx, int device);
+/* As qbc_index_build, with the label rows filled on the GPU `device` (elimination and tree on the
+ * host; the rows, one launch per tree depth, on the device) and left there: the index is uploaded on
+ * return and the host holds no label rows until qbc_index_export or qbc_index_release_device copies
+ * them back.  Same rows as qbc_index_build (TreeDecomp.cpp:388-450 semantics).  Replaces the CPU
+ * label build of TreeDecomp::MakeIndex (TreeDecomp.cpp:388-511) and buildIndex.cpp:246-270. */
+int qbc_index_build_device(const qbc_graph *g, int kind, const int32_t *node_order, int device, qbc_index **out);
 /* drops the device copy (keeps the host index) */
 int qbc_index_release_device(qbc_index *idx);
 /* info[0]=n, [1]=arcs, [2]=label entries, [3]=tree height, [4]=tree width, [5]=device bytes,

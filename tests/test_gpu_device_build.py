@@ -1,0 +1,71 @@
+"""GPU: label rows filled on the device (qbc_index_build_device) equal the host builder's rows
+bit-for-bit (dist, count bits, hop, ancestor ids), for MHL and H2H indexes, and give the same BC."""
+import os
+
+import numpy as np
+import pytest
+
+import gpu_betweennesscentrality_b200 as Q
+import pyoracle as O
+from conftest import GOLDEN, rel_err
+from gpu_betweennesscentrality_b200 import synth
+from util import BC_RTOL, grid_lines
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("vid_of", "depth", "send", "lab_off", "dis", "anc")
+
+
+def _pair(n, u, v, w, kind=Q.QBC_INDEX_MHL, order=None):
+    g = Q.Graph(device=0)
+    g.ReadLines(n, u, v, w)
+    host = g.build_index(kind, order, upload=False)
+    dev = g.build_index(kind, order, on_device=True)
+    return host, dev
+
+
+def _same_rows(host, dev):
+    a, b = host.export(), dev.export()
+    for f in FIELDS:
+        assert np.array_equal(a[f], b[f]), f
+    if a["ch"] is not None:
+        assert np.array_equal(a["ch"], b["ch"])
+
+
+def test_mhl_rows_2k():
+    n, u, v, w = synth.read_graph_lines(os.path.join(GOLDEN, "g2k.txt"))
+    host, dev = _pair(n, u, v, w)
+    bc = dev.bc_all()  # before export: rows only on the device
+    _same_rows(host, dev)
+    assert rel_err(bc, O.TreeCount(n, u, v, w).bc(O.Arcs(n, u, v, w))) <= BC_RTOL
+
+
+def test_h2h_rows_2k():
+    n, u, v, w = synth.read_graph_lines(os.path.join(GOLDEN, "g2k.txt"))
+    order = Q.read_order(os.path.join(GOLDEN, "g2k.order"), n)
+    host, dev = _pair(n, u, v, w, Q.QBC_INDEX_H2H, order)
+    bc = dev.bc_all()
+    _same_rows(host, dev)
+    assert rel_err(bc, O.H2H(O.Arcs(n, u, v, w), order).bc()) <= BC_RTOL
+
+
+@pytest.mark.parametrize("n_target,seed,sc", [(3000, 6, 0.02), (20000, 3, 0.0)])
+def test_mhl_rows_generated(n_target, seed, sc):
+    n, u, v, w = grid_lines(n_target, seed=seed, shortcut_frac=sc)
+    host, dev = _pair(n, u, v, w)
+    srcs = np.arange(0, n, max(1, n // 40), dtype=np.int32)
+    got = dev.bc_sources(srcs)
+    _same_rows(host, dev)
+    host.upload(0)
+    assert rel_err(got, host.bc_sources(srcs)) <= BC_RTOL
+
+
+def test_release_and_reupload_keeps_rows():
+    n, u, v, w = grid_lines(800, seed=2)
+    g = Q.Graph(device=0)
+    g.ReadLines(n, u, v, w)
+    dev = g.build_index(on_device=True)
+    a = dev.bc_all()
+    dev.release_device()  # rows come back to the host first
+    dev.upload(0)
+    assert rel_err(dev.bc_all(), a) <= BC_RTOL
