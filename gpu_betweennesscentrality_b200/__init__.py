@@ -95,6 +95,24 @@ class Index:
         if device is not None and not on_device:
             self.upload(device)
 
+    @classmethod
+    def load(cls, path: str, device: Optional[int] = 0) -> "Index":
+        """Index saved by ``save`` (on-disk format of ``qbc_index_save``), uploaded to ``device``."""
+        self = cls.__new__(cls)
+        self._graph = None
+        h = C.c_void_p()
+        check(lib().qbc_index_load(str(path).encode(), C.byref(h)))
+        self.h = h
+        info = self.info()
+        self.n = int(info[0])
+        self.kind = int(info[6])
+        if device is not None:
+            self.upload(device)
+        return self
+
+    def save(self, path: str) -> None:
+        check(lib().qbc_index_save(self.h, str(path).encode()))
+
     def __del__(self):
         if getattr(self, "h", None):
             try:

@@ -37,6 +37,8 @@ SIGNATURES = {
     "qbc_min_degree_order": (C.c_int, [vp, i32p]),
     "qbc_index_build": (C.c_int, [vp, C.c_int, i32p, C.c_int, C.POINTER(vp)]),
     "qbc_index_upload": (C.c_int, [vp, C.c_int]),
+    "qbc_index_save": (C.c_int, [vp, C.c_char_p]),
+    "qbc_index_load": (C.c_int, [C.c_char_p, C.POINTER(vp)]),
     "qbc_index_build_device": (C.c_int, [vp, C.c_int, i32p, C.c_int, C.POINTER(vp)]),
     "qbc_index_release_device": (C.c_int, [vp]),
     "qbc_index_info": (C.c_int, [vp, i64p]),

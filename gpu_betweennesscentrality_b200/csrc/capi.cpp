@@ -155,6 +155,26 @@ int qbc_index_build_device(const qbc_graph *g, int kind, const int32_t *node_ord
   });
 }
 
+int qbc_index_save(qbc_index *idx, const char *path) {
+  return guarded([&] {
+    need(idx && path, "null argument");
+    if (!idx->h.host.rows_on_host) {
+      not_serving(idx);
+      qbc::device_download_rows(idx->h);
+    }
+    qbc::index_save(idx->h.host, path);
+  });
+}
+
+int qbc_index_load(const char *path, qbc_index **out) {
+  return guarded([&] {
+    need(path && out, "null argument");
+    auto p = std::make_unique<qbc_index>();
+    p->h.host = qbc::index_load(path);
+    *out = p.release();
+  });
+}
+
 int qbc_index_upload(qbc_index *idx, int device) {
   return guarded([&] {
     need(idx, "null index");

@@ -80,4 +80,8 @@ int64_t scan_entries(const Index &ix, const int32_t *sources0, int32_t ns);
 
 int hardware_threads(int requested);
 
+// On-disk index (index_file.cpp): the host index, rows included, with a header and a checksum.
+void index_save(const Index &ix, const std::string &path);
+Index index_load(const std::string &path);
+
 }  // namespace qbc

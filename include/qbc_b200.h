@@ -71,6 +71,12 @@ int qbc_min_degree_order(const qbc_graph *g, int32_t *node_order);
 int qbc_index_build(const qbc_graph *g, int kind, const int32_t *node_order, int nthreads, qbc_index **out);
 /* copies the index to HBM of `device` (cudaSetDevice semantics, QBC.cu:601-602) */
 int qbc_index_upload(qbc_index *idx, int device);
+/* On-disk index (replaces the reference's headerless tmpRoadCountIndex file, TreeDecomp.cpp:243,
+ * 460-467,496-506, and TreeQuery::ReadIndex, TreeDecomp.cpp:748-900): the whole index with its rows,
+ * a versioned header and a checksum.  save copies device-built rows back first; load returns a
+ * host index (then qbc_index_upload).  A damaged, truncated or foreign file gives QBC_EIO. */
+int qbc_index_save(qbc_index *idx, const char *path);
+int qbc_index_load(const char *path, qbc_index **out);
 /* As qbc_index_build, with the label rows filled on the GPU `device` (elimination and tree on the
  * host; the rows, one launch per tree depth, on the device) and left there: the index is uploaded on
  * return and the host holds no label rows until qbc_index_export or qbc_index_release_device copies

@@ -69,3 +69,19 @@ def test_release_and_reupload_keeps_rows():
     dev.release_device()  # rows come back to the host first
     dev.upload(0)
     assert rel_err(dev.bc_all(), a) <= BC_RTOL
+
+
+def test_saved_device_index_cold_start(tmp_path):
+    """a device-built index saved to disk and loaded back serves the same BC (no rebuild)"""
+    n, u, v, w = grid_lines(2000, seed=5)
+    g = Q.Graph(device=0)
+    g.ReadLines(n, u, v, w)
+    dev = g.build_index(on_device=True)
+    a = dev.bc_all()
+    p = str(tmp_path / "dev.qbcidx")
+    dev.save(p)
+    back = Q.Index.load(p, device=0)
+    assert rel_err(back.bc_all(), a) <= BC_RTOL
+    with back.serve() as srv:
+        pts = np.array([0, n // 2, n - 1], np.int32)
+        assert rel_err(srv.wait(srv.submit(pts), 60.0)[0], a[pts]) <= BC_RTOL

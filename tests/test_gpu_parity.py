@@ -251,6 +251,13 @@ def test_cli_drop_in(tmp_path):
                         str(std)], capture_output=True, text=True, env=env, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "BC value is correct" in r.stdout
+    # a tighter tolerance through QBC_STD_TOL, and a planted error it catches
+    bad = tmp_path / "bad.txt"
+    bad.write_text(f"{n} {u.shape[0]}\n" + "".join(f"{i + 1} {x + (1e-6 if i == 5 else 0):.17g}\n" for i, x in enumerate(ref)))
+    env2 = dict(env, QBC_STD_TOL="1e-8")
+    r = subprocess.run([os.path.join(binp, "QBC"), g, os.path.join(GOLDEN, "g2k.order"), "0", str(tmp_path / "q2.txt"),
+                        str(bad)], capture_output=True, text=True, env=env2, timeout=300)
+    assert r.returncode == 1 and "not correct for node 5" in r.stdout
     r = subprocess.run([os.path.join(binp, "RQ"), g, os.path.join(GOLDEN, "g2k.query"), "0"], capture_output=True,
                        text=True, timeout=300)
     assert r.returncode == 0, r.stderr
