@@ -293,12 +293,12 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
     CK(cudaMemcpy(d_tids, tids.data(), tids.size() * 4, cudaMemcpyHostToDevice));
     const int32_t cnt = (int32_t)tids.size();
     Tuning best = h.tuning;
-    double best_t = time_sample(h, d, d_tids, cnt, 2);
+    double best_t = time_sample(h, d, d_tids, cnt, 3);
     auto trial = [&](const Tuning &t) {
       h.tuning = t;
       try {
         if (t.chunk != d->chunk) device_set_chunk(h, t.chunk);
-        const double x = time_sample(h, d, d_tids, cnt, 2);
+        const double x = time_sample(h, d, d_tids, cnt, 3);
         if (x < best_t) {
           best_t = x;
           best = t;
@@ -313,6 +313,17 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
       }
     };
     best.chunk = d->chunk;
+    auto chunk_trials = [&] {
+      for (int32_t ch : {1024, 2048, 4096, 8192}) {
+        if (ch > std::max<int32_t>(32, (cnt + 31) / 32 * 32)) continue;  // the sample must span a chunk
+        if (ch == best.chunk) continue;
+        Tuning t = best;
+        t.chunk = ch;
+        trial(t);
+      }
+    };
+    // 0. sources per scratch buffer (again at the end, after the kernels are chosen)
+    chunk_trials();
     // 1. label kernel: the packed-key kernel with 8 or 16 warps (0 lanes), or the general kernel
     //    with 32/K sources per CTA and 128 or 256 threads
     if (d->packed_bits)
@@ -351,12 +362,7 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
       trial(t);
     }
     // 4. sources per scratch buffer
-    for (int32_t ch : {1024, 2048, 4096, 8192}) {
-      if (ch > std::max<int32_t>(32, (cnt + 31) / 32 * 32)) continue;  // the sample must span a chunk
-      Tuning t = best;
-      t.chunk = ch;
-      trial(t);
-    }
+    chunk_trials();
     h.tuning = best;
     if (d->chunk != best.chunk) device_set_chunk(h, best.chunk);
     *ms_per_source = best_t;
