@@ -57,6 +57,7 @@ struct RowView {
 // ------------------------------------------------------------------------------- K1 + K2
 struct LabelArgs {
   const int32_t *__restrict__ dis;
+  const int32_t *__restrict__ dis_sh;  // dis << bits (packed kernel: keys and target rows pre-shifted)
   const int2 *__restrict__ ch;
   const int32_t *__restrict__ anc;
   const int64_t *__restrict__ lab_off;
@@ -247,8 +248,9 @@ __global__ void __launch_bounds__(256, 1) k_label_scan(LabelArgs a) {
 }
 
 // Packed-key label scan (K=1, 32 sources per CTA).  Each source entry is stored as the key
-// (dist << B) | j and each target entry is shifted by B on the fly, so one shift-add gives
-// (d_s+d_t, j) and a running unsigned min yields the distance and the smallest minimising j at
+// (dist << B) | j and target rows are read from a copy of the label distances pre-shifted by B
+// (dis_sh), so one add gives (d_s+d_t, j) and a running unsigned min yields the distance and the
+// smallest minimising j at
 // once; a second min over key ^ (2^B-1) yields the largest minimising j, so a tie exists iff the two
 // differ.  Valid when every row has at most 2^B entries and 2*max_label < 2^(32-B) - 1 (checked
 // on the host).  Target rows arrive by 1-D TMA bulk copies (cp.async.bulk, no multicast) into two
@@ -325,7 +327,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
   for (int idx = threadIdx.x; idx < G * S; idx += blockDim.x) {
     const int i = idx / S, j = idx - i * S;
     uint32_t key = 0xffffffffu;
-    if (i < gcount && j < s_h[i]) key = ((uint32_t)a.dis[s_off[i] + j] << B) | (uint32_t)j;  // j < S
+    if (i < gcount && j < s_h[i]) key = (uint32_t)a.dis_sh[s_off[i] + j] | (uint32_t)j;  // j < S
     s_key[idx] = key;
   }
   __syncthreads();
@@ -352,7 +354,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
     if (lane == 0) {
       const uint32_t b = issued % kRowBuffers;
       const uint32_t bytes = (uint32_t)(min((a.depth[t] + 3) & ~3, S) * 4);  // S is a multiple of 4
-      bulk_row_to_smem(tb0 + b * S, a.dis + a.lab_off[t], bytes, &s_bar[warp][b]);
+      bulk_row_to_smem(tb0 + b * S, a.dis_sh + a.lab_off[t], bytes, &s_bar[warp][b]);
     }
     issued++;
     if (++next_k == 8) { next_k = 0; next_c += nwarps; }
@@ -410,9 +412,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
         const uint4 y = *reinterpret_cast<const uint4 *>(tbuf + j);
         const uint4 x2 = *reinterpret_cast<const uint4 *>(srow + j + 4);
         const uint4 y2 = *reinterpret_cast<const uint4 *>(tbuf + j + 4);
-        const uint32_t v0 = x.x + (y.x << B), v1 = x.y + (y.y << B), v2 = x.z + (y.z << B), v3 = x.w + (y.w << B);
-        const uint32_t u0 = x2.x + (y2.x << B), u1 = x2.y + (y2.y << B), u2 = x2.z + (y2.z << B),
-                       u3 = x2.w + (y2.w << B);
+        const uint32_t v0 = x.x + y.x, v1 = x.y + y.y, v2 = x.z + y.z, v3 = x.w + y.w;
+        const uint32_t u0 = x2.x + y2.x, u1 = x2.y + y2.y, u2 = x2.z + y2.z, u3 = x2.w + y2.w;
         m1 = __vimin3_u32(m1, v0, v1);
         n1 = __vimin3_u32(n1, u0, u1);
         m1 = __vimin3_u32(m1, v2, v3);
@@ -425,10 +426,10 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
       for (; j < hm; j += 4) {
         const uint4 x = *reinterpret_cast<const uint4 *>(srow + j);
         const uint4 y = *reinterpret_cast<const uint4 *>(tbuf + j);
-        const uint32_t v0 = x.x + (y.x << B);
-        const uint32_t v1 = (j + 1 < hm) ? x.y + (y.y << B) : 0xffffffffu;
-        const uint32_t v2 = (j + 2 < hm) ? x.z + (y.z << B) : 0xffffffffu;
-        const uint32_t v3 = (j + 3 < hm) ? x.w + (y.w << B) : 0xffffffffu;
+        const uint32_t v0 = x.x + y.x;
+        const uint32_t v1 = (j + 1 < hm) ? x.y + y.y : 0xffffffffu;
+        const uint32_t v2 = (j + 2 < hm) ? x.z + y.z : 0xffffffffu;
+        const uint32_t v3 = (j + 3 < hm) ? x.w + y.w : 0xffffffffu;
         m1 = __vimin3_u32(m1, v0, v1);
         m1 = __vimin3_u32(m1, v2, v3);
         m2 = __vimin3_u32(m2, v0 ^ mask, (j + 1 < hm) ? v1 ^ mask : 0xffffffffu);
@@ -436,12 +437,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
       }
       const int64_t toff_t = (hl > S) ? a.lab_off[t] : 0;
       for (j = S; j < hl; j += 4) {  // beyond the shared rows: both rows from global memory
-        const uint4 x = __ldg(reinterpret_cast<const uint4 *>(a.dis + soff + j));
-        const uint4 y = __ldg(reinterpret_cast<const uint4 *>(a.dis + toff_t + j));
-        const uint32_t v0 = (((uint32_t)x.x + (uint32_t)y.x) << B) | (uint32_t)j;
-        const uint32_t v1 = (j + 1 < hl) ? ((((uint32_t)x.y + (uint32_t)y.y) << B) | (uint32_t)(j + 1)) : 0xffffffffu;
-        const uint32_t v2 = (j + 2 < hl) ? ((((uint32_t)x.z + (uint32_t)y.z) << B) | (uint32_t)(j + 2)) : 0xffffffffu;
-        const uint32_t v3 = (j + 3 < hl) ? ((((uint32_t)x.w + (uint32_t)y.w) << B) | (uint32_t)(j + 3)) : 0xffffffffu;
+        const uint4 x = __ldg(reinterpret_cast<const uint4 *>(a.dis_sh + soff + j));
+        const uint4 y = __ldg(reinterpret_cast<const uint4 *>(a.dis_sh + toff_t + j));
+        const uint32_t v0 = (x.x + y.x) | (uint32_t)j;
+        const uint32_t v1 = (j + 1 < hl) ? ((x.y + y.y) | (uint32_t)(j + 1)) : 0xffffffffu;
+        const uint32_t v2 = (j + 2 < hl) ? ((x.z + y.z) | (uint32_t)(j + 2)) : 0xffffffffu;
+        const uint32_t v3 = (j + 3 < hl) ? ((x.w + y.w) | (uint32_t)(j + 3)) : 0xffffffffu;
         m1 = __vimin3_u32(m1, v0, v1);
         m1 = __vimin3_u32(m1, v2, v3);
         m2 = __vimin3_u32(m2, v0 ^ mask, (j + 1 < hl) ? v1 ^ mask : 0xffffffffu);
@@ -460,8 +461,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
           unsigned cc = 0;
           int hh = 0;
           for (int q = 0; q < hl; q++) {
-            const uint32_t dq = q < S ? (srow[q] + ((uint32_t)tbuf[q] << B)) >> B
-                                      : (uint32_t)(__ldg(a.dis + soff + q) + __ldg(a.dis + toff + q));
+            const uint32_t dq = q < S ? (srow[q] + (uint32_t)tbuf[q]) >> B
+                                      : ((uint32_t)__ldg(a.dis_sh + soff + q) + (uint32_t)__ldg(a.dis_sh + toff + q)) >> B;
             if (dq == dist) {
               const int2 cs = __ldg(a.ch + soff + q), ct = __ldg(a.ch + toff + q);
               cc += (unsigned)cs.x * (unsigned)ct.x;
@@ -1129,6 +1130,7 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t
   LabelPlan p = packed ? LabelPlan{1, 32, d->hmax_pad, 512, 1, 0} : plan_label(h, d, ns, plain);
   LabelArgs a{};
   a.dis = d->dis;
+  a.dis_sh = d->dis_sh;
   a.ch = d->ch;
   a.anc = d->anc;
   a.lab_off = d->lab_off;
@@ -1365,6 +1367,11 @@ __global__ void __launch_bounds__(256) k_fill_level(FillArgs f, const int32_t *_
   }
 }
 
+__global__ void k_shift_left(const int32_t *__restrict__ in, int32_t *__restrict__ out, int64_t n, int bits) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (int32_t)((uint32_t)in[i] << bits);
+}
+
 __global__ void k_max_i32(const int32_t *__restrict__ x, int64_t n, int32_t *out) {
   int m = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) m = max(m, x[i]);
@@ -1422,6 +1429,12 @@ static void finish_state(Handle &h, DeviceState *d) {
     while ((1 << B) < ix.tree_height) B++;
     const uint64_t room = (uint64_t)1 << (32 - B);
     d->packed_bits = (B <= 16 && 2ull * (uint64_t)std::max(ix.max_label, 0) + 2 < room) ? B : 0;
+  }
+  if (d->packed_bits) {  // label distances pre-shifted by B for the packed kernel (one add per entry)
+    const int64_t L = ix.lab_off[ix.n];
+    d->dis_sh = dmalloc<int32_t>(d, (size_t)L);
+    k_shift_left<<<148 * 8, 256, 0, st>>>(d->dis, d->dis_sh, L, d->packed_bits);
+    CK(cudaGetLastError());
   }
   alloc_scratch(h, d);
   d->bc_tid = dmalloc<double>(d, ix.n);
@@ -1559,7 +1572,7 @@ void device_release(Handle &h) {
   cudaSetDevice(d->device);
   cudaDeviceSynchronize();
   void *ptrs[] = {d->depth, d->send, d->arc_off, d->arc_head, d->arc_w, d->arc_rng, d->arc_hw, d->vid_of, d->tid_of, d->lab_off, d->dis,
-                  d->anc, d->aend, d->ch, d->bc_tid, d->bc_vid, d->err, d->sources};
+                  d->dis_sh, d->anc, d->aend, d->ch, d->bc_tid, d->bc_vid, d->err, d->sources};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   free_scratch(d);

@@ -35,6 +35,7 @@ struct DeviceState {
   int2 *arc_rng = nullptr, *arc_hw = nullptr;
   int32_t *vid_of = nullptr, *tid_of = nullptr, *dis = nullptr, *anc = nullptr, *aend = nullptr;
   int32_t packed_bits = 0;  // > 0: the packed-key label scan applies
+  int32_t *dis_sh = nullptr;  // dis << packed_bits (packed kernel only)
   int64_t *lab_off = nullptr;
   int2 *ch = nullptr;
   // scratch: one buffer of `chunk` source slots (index 1 unused)
