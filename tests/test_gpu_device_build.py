@@ -85,3 +85,15 @@ def test_saved_device_index_cold_start(tmp_path):
     with back.serve() as srv:
         pts = np.array([0, n // 2, n - 1], np.int32)
         assert rel_err(srv.wait(srv.submit(pts), 60.0)[0], a[pts]) <= BC_RTOL
+
+
+@pytest.mark.parametrize("name", ["single", "pair", "path3", "star5", "cycle4", "path40"])
+def test_known_graphs_device_build(name):
+    from util import KNOWN, lines_of
+
+    n, edges, expect = KNOWN[name]
+    nn, u, v, w = lines_of(edges, n)
+    host, dev = _pair(nn, u, v, w)
+    bc = dev.bc_all()
+    _same_rows(host, dev)
+    assert np.allclose(bc, expect, rtol=0, atol=1e-9)

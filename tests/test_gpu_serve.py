@@ -191,3 +191,23 @@ def test_poisson_load_2k(g2k):
             assert rel_err(vals, full[s]) <= BC_RTOL
     finally:
         idx.set_tuning()
+
+
+@pytest.mark.parametrize("name", ["single", "pair", "path3", "star5", "path40"])
+def test_batch_and_serve_on_small_graphs(name):
+    from util import KNOWN, lines_of
+
+    n, edges, expect = KNOWN[name]
+    nn, u, v, w = lines_of(edges, n)
+    g = Q.Graph(device=0)
+    g.ReadLines(nn, u, v, w)
+    idx = g.build_index()
+    want = np.asarray(expect, np.float64)
+    sets = [np.arange(n, dtype=np.int32), np.array([n - 1], np.int32), np.zeros(0, np.int32)]
+    outs = idx.bc_query_batch(sets)
+    for s_, o in zip(sets, outs):
+        assert np.allclose(o, want[s_], rtol=0, atol=1e-9)
+    with idx.serve(max_active=2) as srv:
+        ts = [srv.submit(s_) for s_ in sets]
+        for s_, t in zip(sets, ts):
+            assert np.allclose(srv.wait(t, 60.0)[0], want[s_], rtol=0, atol=1e-9)
