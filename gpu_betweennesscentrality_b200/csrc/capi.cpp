@@ -245,7 +245,7 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
     need(idx && (nparams == 0 || params), "null argument");
     qbc::Tuning &t = idx->h.tuning;
     not_serving(idx);
-    int32_t *f[] = {&t.lanes_per_source, &t.label_threads, &t.split, &t.chunk, &t.dep_threads, &t.dep_form, &t.queue_depth, &t.label_warps, &t.label_tile};
+    int32_t *f[] = {&t.lanes_per_source, &t.label_threads, &t.split, &t.chunk, &t.dep_threads, &t.dep_form, &t.queue_depth, &t.label_warps, &t.label_tile, &t.label_passes};
     if (nparams > 0) {
       int32_t k = params[0];
       need(k == 0 || k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32, "lanes per source must be 0 or a power of two <= 32");
@@ -255,7 +255,8 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
     if (nparams > 6) need(params[6] == 0 || (params[6] >= 64 && params[6] <= 2048), "queue depth must be 0 or in [64, 2048]");
     if (nparams > 7) need(params[7] == 0 || params[7] == 8 || params[7] == 16, "label warps must be 0, 8 or 16");
     if (nparams > 8) need(params[8] >= 0, "label tile must be >= 0");
-    for (int32_t i = 0; i < nparams && i < 9; i++) *f[i] = params[i];
+    if (nparams > 9) need(params[9] >= 0 && params[9] <= 2, "label passes must be 0, 1 or 2");
+    for (int32_t i = 0; i < nparams && i < 10; i++) *f[i] = params[i];
     if (nparams > 3 && t.chunk != old_chunk && idx->h.dev) qbc::device_set_chunk(idx->h, t.chunk);
   });
 }
@@ -264,8 +265,8 @@ int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams)
   return guarded([&] {
     need(idx && (nparams == 0 || params), "null argument");
     const qbc::Tuning &t = idx->h.tuning;
-    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile};
-    for (int32_t i = 0; i < nparams && i < 9; i++) params[i] = f[i];
+    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes};
+    for (int32_t i = 0; i < nparams && i < 10; i++) params[i] = f[i];
   });
 }
 
@@ -353,8 +354,8 @@ int qbc_autotune(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *p
     qbc::autotune(idx->h, sources0, ns, &ms);
     if (ms_per_source) *ms_per_source = ms;
     const qbc::Tuning &t = idx->h.tuning;
-    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile};
-    for (int32_t i = 0; params && i < nparams && i < 9; i++) params[i] = f[i];
+    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes};
+    for (int32_t i = 0; params && i < nparams && i < 10; i++) params[i] = f[i];
   });
 }
 

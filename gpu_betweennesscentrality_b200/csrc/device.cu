@@ -70,6 +70,9 @@ struct LabelArgs {
   int32_t *__restrict__ maxhop;   // [ns] largest hop layer per source (atomicMax), or null
   const int32_t *__restrict__ aend;  // subtree end of each row entry's ancestor (packed kernel)
   int32_t bits;                      // index bits of the packed keys (packed kernel)
+  int32_t pass_lo;                   // multi-pass packed kernel: first row entry of this pass's tile
+  int32_t multipass;                 // 1: rows longer than the tile take several passes (state in
+                                     //    out_rec between passes); 0: entries beyond the tile from global
   int32_t *err;                      // device error word (packed kernel's bounded waits)
 };
 
@@ -314,20 +317,28 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
   if (first >= a.ns) return;
   const int gcount = min(G, a.ns - first);
   const uint32_t B = (uint32_t)a.bits, mask = (1u << B) - 1u;
+  __shared__ int32_t s_hmax;
   if (threadIdx.x < G) {
     const int i = threadIdx.x;
     const int s = i < gcount ? a.src[first + i] : 0;
     s_h[i] = i < gcount ? a.depth[s] : 0;
     s_off[i] = a.lab_off[s];
+    const int hm32 = __reduce_max_sync(kFull, s_h[i]);
+    if (i == 0) s_hmax = hm32;
   }
   if (lane == 0)
     for (int b = 0; b < kRowBuffers; b++) mbar_init(&s_bar[warp][b], 1);
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   __syncthreads();
+  // Multi-pass: this pass scans row entries [P0, P0 + S); a CTA whose rows all ended in an earlier
+  // pass has nothing left, and the pass that reaches its deepest row finalises its pairs.
+  const int P0 = a.multipass ? a.pass_lo : 0;
+  if (a.multipass && P0 > 0 && s_hmax <= P0) return;
+  const bool fin = !a.multipass || s_hmax <= P0 + S;
   for (int idx = threadIdx.x; idx < G * S; idx += blockDim.x) {
-    const int i = idx / S, j = idx - i * S;
+    const int i = idx / S, jj = idx - i * S, j = P0 + jj;
     uint32_t key = 0xffffffffu;
-    if (i < gcount && j < s_h[i]) key = (uint32_t)a.dis_sh[s_off[i] + j] | (uint32_t)j;  // j < S
+    if (i < gcount && j < s_h[i]) key = (uint32_t)a.dis_sh[s_off[i] + j] | (uint32_t)j;
     s_key[idx] = key;
   }
   __syncthreads();
@@ -353,8 +364,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
     if (t >= a.n) { next_c = cend; return; }
     if (lane == 0) {
       const uint32_t b = issued % kRowBuffers;
-      const uint32_t bytes = (uint32_t)(min((a.depth[t] + 3) & ~3, S) * 4);  // S is a multiple of 4
-      bulk_row_to_smem(tb0 + b * S, a.dis_sh + a.lab_off[t], bytes, &s_bar[warp][b]);
+      // entries [P0, P0 + S) of the row (S and P0 are multiples of 4: 16-byte aligned); a row that
+      // ends before P0 is not scanned in this pass, 16 bytes of its start are copied instead
+      const int rem = ((a.depth[t] + 3) & ~3) - P0;
+      const int64_t src = a.lab_off[t] + (rem > 0 ? P0 : 0);
+      const uint32_t bytes = (uint32_t)((rem > 0 ? min(rem, S) : 4) * 4);
+      bulk_row_to_smem(tb0 + b * S, a.dis_sh + src, bytes, &s_bar[warp][b]);
     }
     issued++;
     if (++next_k == 8) { next_k = 0; next_c += nwarps; }
@@ -380,6 +395,15 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
     int loN = (have && J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
     uint32_t pending = 0;  // targets whose counts are gathered after the chunk
     const int kend = min(8, a.n - t0);
+    if (a.multipass && P0 > 0) {  // (m1, m2) of the earlier passes, kept in the output records
+      const int4 *grec = a.out_rec + blk(first, t0, a.ns);
+      int2 *sdc_all = reinterpret_cast<int2 *>(sdc);
+      for (int p = lane; p < gcount * 8; p += 32) {
+        const int4 x = grec[p];
+        sdc_all[(p >> 3) * 10 + (p & 7)] = make_int2(x.x, x.y);
+      }
+      __syncwarp();
+    }
     for (int k = 0; k < kend; k++) {
       const int t = t0 + k;
       // advance the interval: targets grow, so t leaves intervals on the right and enters a deeper
@@ -403,8 +427,13 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
       done++;
       const int32_t *tbuf = tb0 + b * S;
       const int hl = have ? J + 1 : 0;
-      const int hm = min(hl, S);  // entries held in shared memory
+      const int hm = max(0, min(hl, P0 + S) - P0);  // entries of this pass held in shared memory
       uint32_t m1 = 0xffffffffu, m2 = 0xffffffffu, n1 = 0xffffffffu, n2 = 0xffffffffu;
+      if (a.multipass && P0 > 0 && have) {
+        const int2 st = sdc2[k];
+        m1 = (uint32_t)st.x;
+        m2 = (uint32_t)st.y;
+      }
       const int full8 = hm & ~7;
       int j = 0;
       for (; j < full8; j += 8) {
@@ -435,8 +464,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
         m2 = __vimin3_u32(m2, v0 ^ mask, (j + 1 < hm) ? v1 ^ mask : 0xffffffffu);
         m2 = __vimin3_u32(m2, (j + 2 < hm) ? v2 ^ mask : 0xffffffffu, (j + 3 < hm) ? v3 ^ mask : 0xffffffffu);
       }
-      const int64_t toff_t = (hl > S) ? a.lab_off[t] : 0;
-      for (j = S; j < hl; j += 4) {  // beyond the shared rows: both rows from global memory
+      const int64_t toff_t = (!a.multipass && hl > S) ? a.lab_off[t] : 0;
+      for (j = S; !a.multipass && j < hl; j += 4) {  // beyond the shared rows: both rows from global memory
         const uint4 x = __ldg(reinterpret_cast<const uint4 *>(a.dis_sh + soff + j));
         const uint4 y = __ldg(reinterpret_cast<const uint4 *>(a.dis_sh + toff_t + j));
         const uint32_t v0 = (x.x + y.x) | (uint32_t)j;
@@ -450,6 +479,11 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
       }
       m1 = min(m1, n1);
       m2 = min(m2, n2);
+      if (!fin) {  // carry (m1, m2) to the next pass
+        if (have) sdc2[k] = make_int2((int)m1, (int)m2);
+        __syncwarp();
+        continue;
+      }
       const uint32_t dist = m1 >> B;
       int cnt = 0, hop = 0;
       if (COUNTS && have) {
@@ -461,8 +495,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
           unsigned cc = 0;
           int hh = 0;
           for (int q = 0; q < hl; q++) {
-            const uint32_t dq = q < S ? (srow[q] + (uint32_t)tbuf[q]) >> B
-                                      : ((uint32_t)__ldg(a.dis_sh + soff + q) + (uint32_t)__ldg(a.dis_sh + toff + q)) >> B;
+            const bool in_tile = q >= P0 && q < P0 + S;
+            const uint32_t dq = in_tile ? (srow[q - P0] + (uint32_t)tbuf[q - P0]) >> B
+                                        : ((uint32_t)__ldg(a.dis_sh + soff + q) + (uint32_t)__ldg(a.dis_sh + toff + q)) >> B;
             if (dq == dist) {
               const int2 cs = __ldg(a.ch + soff + q), ct = __ldg(a.ch + toff + q);
               cc += (unsigned)cs.x * (unsigned)ct.x;
@@ -486,7 +521,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
         if (COUNTS) shp1[k] = 0;
       }
     }
-    if (COUNTS && have && pending) {
+    if (COUNTS && fin && have && pending) {
       int2 cs8[8], ct8[8];
 #pragma unroll
       for (int k = 0; k < 8; k++) {
@@ -504,7 +539,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
         }
       }
     }
-    if (COUNTS && have) {
+    if (COUNTS && fin && have) {
 #pragma unroll
       for (int k = 0; k < 8; k++) mh = max(mh, shp1[k]);
     }
@@ -516,7 +551,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
         const int2 x = sdc_all[(p >> 3) * 10 + (p & 7)];
         grec[p] = make_int4(x.x, x.y, 0, 0);
       }
-      if (COUNTS) {
+      if (COUNTS && fin) {
         int4 *ghp = reinterpret_cast<int4 *>(a.out_hop + blk(first, t0, a.ns));
         for (int p = lane; p < gcount * 2; p += 32) ghp[p] = shp[(p >> 1) * 3 + (p & 1)];
       }
@@ -532,7 +567,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
     }
     return;
   }
-  if (COUNTS && have && a.maxhop) atomicMax(a.maxhop + first + lane, mh);
+  if (COUNTS && fin && have && a.maxhop) atomicMax(a.maxhop + first + lane, mh);
 }
 
 // ------------------------------------------------------------------------------- K3 - K5
@@ -1093,8 +1128,16 @@ static void launch_label_packed_w(const Handle &h, const DeviceState *d, LabelAr
   auto kern = k_label_scan_packed<C, W>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(split, groups);
-  kern<<<grid, W * 32, smem, st>>>(a);
-  CK(cudaGetLastError());
+  // rows longer than the tile: one pass reading the entries beyond the tile from global memory
+  // (default), or several passes over tiles of S entries (label_passes = 2; measured slower at 1M:
+  // every pass re-walks all targets of the CTA, 3.0 vs 4.6 label entries/clk/SM)
+  const int passes = (d->hmax_pad + S - 1) / S;
+  a.multipass = (passes > 1 && h.tuning.label_passes == 2) ? 1 : 0;
+  for (int p = 0; p < (a.multipass ? passes : 1); p++) {
+    a.pass_lo = p * S;
+    kern<<<grid, W * 32, smem, st>>>(a);
+    CK(cudaGetLastError());
+  }
 }
 
 template <bool C>

@@ -107,7 +107,10 @@ int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int3
  * counted in shared memory, 64..2048; 0 = 512), [7]=warps per CTA of the packed-key kernel (8 or
  * 16; 0 = 16 when the whole tree height fits shared memory, else 8), [8]=label tile: entries of
  * each row staged in shared memory by the packed-key kernel (0 = all that fit; later entries of a
- * scan are read from global memory).  Refused with QBC_EBUSY while the index serves. */
+ * scan are read from global memory or taken in further passes, see [9]), [9]=label passes for
+ * rows longer than the tile (0 = 1: one launch, entries beyond the tile read from global memory;
+ * 2: one launch per tile of entries, the pairs' running minima kept in the output rows between
+ * passes).  Refused with QBC_EBUSY while the index serves. */
 int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams);
 int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams);
 
@@ -121,7 +124,7 @@ int qbc_index_stats(qbc_index *idx, double *out);
 /* Autotuner (no counterpart in the reference): times candidate tunings -- sources per CTA and
  * threads of the label kernel, target split, dependency form and level-queue depth, chunk size --
  * on a sweep over the listed sources, keeps the fastest on the index and returns it in params
- * (layout of qbc_index_set_tuning, up to 9) with its time per source in ms. */
+ * (layout of qbc_index_set_tuning, up to 10) with its time per source in ms. */
 int qbc_autotune(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *params, int32_t nparams,
                  double *ms_per_source);
 

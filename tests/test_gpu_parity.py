@@ -59,13 +59,15 @@ def test_rows_identical_across_tunings(g2k, lanes):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("warps,tile", [(16, 0), (8, 0), (16, 32), (8, 48), (16, 8)])
-def test_packed_kernel_tiles_and_warps(g2k, warps, tile):
-    """label entries beyond the shared-memory tile come from global memory: same rows, same BC"""
+@pytest.mark.parametrize("warps,tile,passes", [(16, 0, 0), (8, 0, 0), (16, 32, 1), (8, 48, 1), (16, 8, 1),
+                                               (16, 32, 2), (8, 48, 2), (16, 8, 2), (8, 20, 0)])
+def test_packed_kernel_tiles_and_warps(g2k, warps, tile, passes):
+    """rows longer than the shared-memory tile: several tile passes (state kept in the output rows)
+    or one pass with the entries beyond the tile from global memory: same rows, same BC"""
     n, u, v, w, g, idx, tc, arcs = g2k
     srcs = np.arange(0, n, 11, dtype=np.int32)
     base = idx.rows(srcs)
-    idx.set_tuning(label_warps=warps, label_tile=tile)
+    idx.set_tuning(label_warps=warps, label_tile=tile, label_passes=passes)
     try:
         alt = idx.rows(srcs)
         bc = idx.bc_sources(srcs)
