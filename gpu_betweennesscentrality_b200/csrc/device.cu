@@ -71,8 +71,8 @@ struct LabelArgs {
   const int32_t *__restrict__ aend;  // subtree end of each row entry's ancestor (packed kernel)
   int32_t bits;                      // index bits of the packed keys (packed kernel)
   int32_t pass_lo;                   // multi-pass packed kernel: first row entry of this pass's tile
-  int32_t multipass;                 // 1: rows longer than the tile take several passes (state in
-                                     //    out_rec between passes); 0: entries beyond the tile from global
+  int32_t multipass;                 // launcher only: rows longer than the tile take several passes
+                                     // (kernel variant MP, state in out_rec between passes)
   int32_t *err;                      // device error word (packed kernel's bounded waits)
 };
 
@@ -298,7 +298,7 @@ __host__ __device__ constexpr size_t packed_smem(int warps, int S) {
 
 // Rows are held in shared memory up to S entries (S = the padded tree height when it fits);
 // entries j >= S of a scan (taller trees) are read from global memory, 4 at a time.
-template <bool COUNTS, int WARPS>
+template <bool COUNTS, int WARPS, bool MP>
 __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a) {
   constexpr int G = 32;
   extern __shared__ int4 smem4[];
@@ -332,9 +332,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
   __syncthreads();
   // Multi-pass: this pass scans row entries [P0, P0 + S); a CTA whose rows all ended in an earlier
   // pass has nothing left, and the pass that reaches its deepest row finalises its pairs.
-  const int P0 = a.multipass ? a.pass_lo : 0;
-  if (a.multipass && P0 > 0 && s_hmax <= P0) return;
-  const bool fin = !a.multipass || s_hmax <= P0 + S;
+  const int P0 = MP ? a.pass_lo : 0;
+  if (MP && P0 > 0 && s_hmax <= P0) return;
+  const bool fin = !MP || s_hmax <= P0 + S;
   for (int idx = threadIdx.x; idx < G * S; idx += blockDim.x) {
     const int i = idx / S, jj = idx - i * S, j = P0 + jj;
     uint32_t key = 0xffffffffu;
@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
     int loN = (have && J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
     uint32_t pending = 0;  // targets whose counts are gathered after the chunk
     const int kend = min(8, a.n - t0);
-    if (a.multipass && P0 > 0) {  // (m1, m2) of the earlier passes, kept in the output records
+    if (MP && P0 > 0) {  // (m1, m2) of the earlier passes, kept in the output records
       const int4 *grec = a.out_rec + blk(first, t0, a.ns);
       int2 *sdc_all = reinterpret_cast<int2 *>(sdc);
       for (int p = lane; p < gcount * 8; p += 32) {
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
       const int hl = have ? J + 1 : 0;
       const int hm = max(0, min(hl, P0 + S) - P0);  // entries of this pass held in shared memory
       uint32_t m1 = 0xffffffffu, m2 = 0xffffffffu, n1 = 0xffffffffu, n2 = 0xffffffffu;
-      if (a.multipass && P0 > 0 && have) {
+      if (MP && P0 > 0 && have) {
         const int2 st = sdc2[k];
         m1 = (uint32_t)st.x;
         m2 = (uint32_t)st.y;
@@ -464,8 +464,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
         m2 = __vimin3_u32(m2, v0 ^ mask, (j + 1 < hm) ? v1 ^ mask : 0xffffffffu);
         m2 = __vimin3_u32(m2, (j + 2 < hm) ? v2 ^ mask : 0xffffffffu, (j + 3 < hm) ? v3 ^ mask : 0xffffffffu);
       }
-      const int64_t toff_t = (!a.multipass && hl > S) ? a.lab_off[t] : 0;
-      for (j = S; !a.multipass && j < hl; j += 4) {  // beyond the shared rows: both rows from global memory
+      const int64_t toff_t = (!MP && hl > S) ? a.lab_off[t] : 0;
+      for (j = S; !MP && j < hl; j += 4) {  // beyond the shared rows: both rows from global memory
         const uint4 x = __ldg(reinterpret_cast<const uint4 *>(a.dis_sh + soff + j));
         const uint4 y = __ldg(reinterpret_cast<const uint4 *>(a.dis_sh + toff_t + j));
         const uint32_t v0 = (x.x + y.x) | (uint32_t)j;
@@ -1125,14 +1125,14 @@ static void launch_label_packed_w(const Handle &h, const DeviceState *d, LabelAr
   }
   a.stride = S;
   a.split = split;
-  auto kern = k_label_scan_packed<C, W>;
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(split, groups);
   // rows longer than the tile: one pass reading the entries beyond the tile from global memory
   // (default), or several passes over tiles of S entries (label_passes = 2; measured slower at 1M:
   // every pass re-walks all targets of the CTA, 3.0 vs 4.6 label entries/clk/SM)
   const int passes = (d->hmax_pad + S - 1) / S;
   a.multipass = (passes > 1 && h.tuning.label_passes == 2) ? 1 : 0;
+  auto kern = a.multipass ? k_label_scan_packed<C, W, true> : k_label_scan_packed<C, W, false>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int p = 0; p < (a.multipass ? passes : 1); p++) {
     a.pass_lo = p * S;
     kern<<<grid, W * 32, smem, st>>>(a);
