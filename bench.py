@@ -110,7 +110,7 @@ def run_reference(args):
     import pyoracle
     from gpu_betweennesscentrality_b200 import synth
 
-    path = synth.cached_graph(CACHE, args.n, seed=args.seed)
+    path = synth.cached_graph(CACHE, args.n, seed=args.seed, shortcut_frac=args.shortcuts)
     n, u, v, w = synth.read_graph_lines(path)
     tc = pyoracle.TreeCount(n, u, v, w)
     arcs = pyoracle.Arcs(n, u, v, w)
@@ -139,7 +139,8 @@ def run_reference(args):
            "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
            "scaling": "strong", "vs_baseline": None, "dtype": "int32 dist/count, f64 dependency", "data": "synthetic",
            "impl": "reference",
-           "config": _config(n, int(u.shape[0]) // 2, per_step, args),
+           # the same workload as the B200 arm; each timed step here is a bounded sample of it
+           "config": _config(n, int(u.shape[0]) // 2, args.sample if 0 < args.sample < n else n, args),
            "cpu_baseline": {"value": val, "unit": "sources/s", "cores": cores, "kind": "port", "sample": sample},
            "e2e": {"value": val, "unit": "sources/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
