@@ -251,7 +251,7 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
       need(k == 0 || k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32, "lanes per source must be 0 or a power of two <= 32");
     }
     const int32_t old_chunk = t.chunk;
-    if (nparams > 5) need(params[5] >= 0 && params[5] <= 3, "dependency form must be 0, 1, 2 or 3");
+    if (nparams > 5) need(params[5] >= 0 && params[5] <= 4, "dependency form must be 0..4");
     if (nparams > 6) need(params[6] == 0 || (params[6] >= 64 && params[6] <= 2048), "queue depth must be 0 or in [64, 2048]");
     if (nparams > 7) need(params[7] == 0 || params[7] == 8 || params[7] == 16, "label warps must be 0, 8 or 16");
     if (nparams > 8) need(params[8] >= 0, "label tile must be >= 0");

@@ -763,9 +763,9 @@ __device__ __forceinline__ StepIt step_first(const int *cnt, int maxL) {
   return StepIt{L, L >= 1 ? cnt[L] : 0, L >= 1 ? cnt[L + 1] : 0};
 }
 
-__device__ __forceinline__ StepIt step_next(const int *cnt, StepIt it) {
+__device__ __forceinline__ StepIt step_next(const int *cnt, StepIt it, int width = 32) {
   if (it.L < 1) return it;
-  it.idx += 32;
+  it.idx += width;
   if (it.idx < it.end) return it;
   int L = it.L - 1;
   while (L >= 1 && cnt[L] == cnt[L + 1]) L--;
@@ -921,6 +921,92 @@ __global__ void __launch_bounds__(256, 3) k_dependency_warp(DepArgs a, const int
       }
       __syncwarp();
     }
+  }
+}
+
+// CTA-per-source form with the software-pipelined backprop of k_dependency_warp<true> (steps of
+// blockDim.x vertices, a __syncthreads between layers); the largest layer comes from the label
+// kernel, so the pass over the hop layers that k_dependency makes to find it is skipped.
+__global__ void __launch_bounds__(256, 4) k_dependency_cta_pipe(DepArgs a, const int32_t *__restrict__ maxhop) {
+  __shared__ int sh_cnt[kLayerCap + 2];
+  __shared__ int sh_cur[kLayerCap + 2];
+  __shared__ int red[33];
+  const int slot = blockIdx.x;
+  if (slot >= a.ns) return;
+  const int s = a.src[slot];
+  const size_t base = (size_t)slot * a.n_pad;
+  const RowView<int4> rec{a.rec, slot, a.ns};
+  const RowView<const int32_t> hop{a.hop, slot, a.ns};
+  int32_t *order = a.order + base;
+  const int maxL = maxhop[slot];
+  int *cnt = sh_cnt, *cur = sh_cur;
+  if (maxL + 2 > kLayerCap) {
+    cnt = a.lcnt + (size_t)slot * 2 * (a.n_pad + 2);
+    cur = cnt + (a.n_pad + 2);
+  }
+  for (int i = threadIdx.x; i <= maxL + 1; i += blockDim.x) cnt[i] = 0;
+  __syncthreads();
+  for (int v = threadIdx.x; v < a.n; v += blockDim.x)
+    if (v != s) layer_slot(cnt, hop[v]);
+  __syncthreads();
+  block_exclusive_scan(cnt, maxL + 1, red);
+  for (int i = threadIdx.x; i <= maxL + 1; i += blockDim.x) cur[i] = cnt[i];
+  __syncthreads();
+  for (int v = threadIdx.x; v < a.n; v += blockDim.x)
+    if (v != s) order[layer_slot(cur, hop[v])] = v;
+  __syncthreads();
+  const int W = blockDim.x, tid = threadIdx.x;
+  StepIt itC = step_first(cnt, maxL);
+  StepIt itB = step_next(cnt, itC, W);
+  StepIt itA = step_next(cnt, itB, W);
+  auto vertex_at = [&](const StepIt &it) { return (it.L >= 1 && it.idx + tid < it.end) ? order[it.idx + tid] : -1; };
+  int vC = vertex_at(itC);
+  int4 rC = vC >= 0 ? rec[vC] : make_int4(0, 0, 0, 0);
+  int2 gC = vC >= 0 ? a.arc_rng[vC] : make_int2(0, 0);
+  int2 hC[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) hC[q] = (gC.x + q < gC.y) ? a.arc_hw[gC.x + q] : make_int2(-1, 0);
+  int vB = vertex_at(itB);
+  int4 rB = vB >= 0 ? rec[vB] : make_int4(0, 0, 0, 0);
+  int2 gB = vB >= 0 ? a.arc_rng[vB] : make_int2(0, 0);
+  int vA = vertex_at(itA);
+  while (itC.L >= 1) {
+    int2 hB[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) hB[q] = (gB.x + q < gB.y) ? a.arc_hw[gB.x + q] : make_int2(-1, 0);
+    const int4 rA = vA >= 0 ? rec[vA] : make_int4(0, 0, 0, 0);
+    const int2 gA = vA >= 0 ? a.arc_rng[vA] : make_int2(0, 0);
+    const StepIt itN = step_next(cnt, itA, W);
+    const int vN = vertex_at(itN);
+    if (vC >= 0) {
+      int4 rw[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (hC[q].x >= 0) rw[q] = rec[hC[q].x];
+      double acc = 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (hC[q].x >= 0 && rw[q].x == rC.x + hC[q].y) acc += rec_rho(rw[q]);
+      for (int e = gC.x + 4; e < gC.y; e++) {
+        const int2 hw = a.arc_hw[e];
+        const int4 r = rec[hw.x];
+        if (r.x == rC.x + hw.y) acc += rec_rho(r);
+      }
+      finish_vertex(a, rec, vC, (double)rC.y, acc);
+    }
+    if (itB.L != itC.L) __syncthreads();  // this layer's rho visible to the next
+    itC = itB;
+    vC = vB;
+    rC = rB;
+    gC = gB;
+#pragma unroll
+    for (int q = 0; q < 4; q++) hC[q] = hB[q];
+    itB = itA;
+    vB = vA;
+    rB = rA;
+    gB = gA;
+    itA = itN;
+    vA = vN;
   }
 }
 
@@ -1222,7 +1308,7 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *
                        bool plain = false) {
   DepArgs a = dep_args(d, buf, src, ns);
   const int threads = std::max(64, std::min(256, (h.tuning.dep_threads / 32) * 32));
-  const bool warp_form = h.host.kind == IndexKind::MHL && h.tuning.dep_form != 2 && !plain;
+  const bool warp_form = h.host.kind == IndexKind::MHL && h.tuning.dep_form != 2 && h.tuning.dep_form != 4 && !plain;
   std::pair<cudaEvent_t, cudaEvent_t> ev{};
   if (d->profiling) {
     ev = take_events(d->ev_dp, d->ev_dp_used);
@@ -1240,6 +1326,8 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *
     if (h.tuning.dep_form == 3 || h.tuning.dep_form == 0)
       k_dependency_warp<true><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
     else k_dependency_warp<false><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
+  } else if (h.host.kind == IndexKind::MHL && h.tuning.dep_form == 4) {
+    k_dependency_cta_pipe<<<ns, threads, 0, st>>>(a, d->maxhop[buf]);
   } else if (h.host.kind == IndexKind::MHL) {
     k_dependency<<<ns, threads, 0, st>>>(a);
   } else {

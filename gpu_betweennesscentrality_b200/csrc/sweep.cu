@@ -359,12 +359,13 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
         t.queue_depth = qd;
         trial(t);
       }
-    for (int32_t th : {128, 256}) {
-      Tuning t = best;
-      t.dep_form = 2;
-      t.dep_threads = th;
-      trial(t);
-    }
+    for (int32_t form : {2, 4})
+      for (int32_t th : {128, 256}) {
+        Tuning t = best;
+        t.dep_form = form;
+        t.dep_threads = th;
+        trial(t);
+      }
     // 4. sources per scratch buffer
     chunk_trials();
     h.tuning = best;

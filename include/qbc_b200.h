@@ -103,7 +103,8 @@ int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int3
  * label kernel, [2]=target split per source group (0=auto), [3]=sources per chunk (0=auto),
  * [4]=threads per CTA of the CTA-per-source dependency kernel, [5]=dependency form (0 auto = 3,
  * 1 one warp per source, 2 one CTA per source, 3 one warp per source with the backprop's
- * layer-independent loads issued one to three steps ahead), [6]=level-queue depth of the warp form (layers
+ * layer-independent loads issued one to three steps ahead, 4 one CTA per source, pipelined the
+ * same way), [6]=level-queue depth of the warp form (layers
  * counted in shared memory, 64..2048; 0 = 512), [7]=warps per CTA of the packed-key kernel (8 or
  * 16; 0 = 16 when the whole tree height fits shared memory, else 8), [8]=label tile: entries of
  * each row staged in shared memory by the packed-key kernel (0 = all that fit; later entries of a

@@ -95,7 +95,7 @@ def test_plain_path_matches_batched(g2k):
     assert rel_err(idx.bc_sources(srcs), tc.bc(arcs, srcs)) <= BC_RTOL
 
 
-@pytest.mark.parametrize("form", [1, 2, 3])
+@pytest.mark.parametrize("form", [1, 2, 3, 4])
 def test_dependency_forms_agree(g2k, form):
     n, u, v, w, g, idx, tc, arcs = g2k
     srcs = np.arange(0, n, 5, dtype=np.int32)
@@ -184,7 +184,7 @@ def test_shortcut_graph_rows_and_bc():
         assert np.array_equal(d[k], d0) and np.array_equal(c[k], c0) and np.array_equal(h[k], h0)
     want = tc.bc(O.Arcs(n, u, v, w), srcs)
     try:
-        for form in (0, 1, 2, 3):  # shortcut vertices have more than four arcs
+        for form in (0, 1, 2, 3, 4):  # shortcut vertices have more than four arcs
             idx.set_tuning(dep_form=form, queue_depth=64 if form == 3 else 0)
             assert rel_err(idx.bc_sources(srcs), want) <= BC_RTOL, form
     finally:
