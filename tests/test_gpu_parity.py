@@ -10,7 +10,7 @@ import gpu_betweennesscentrality_b200 as Q
 import pyoracle as O
 from conftest import GOLDEN, ROOT, rel_err
 from gpu_betweennesscentrality_b200 import synth
-from util import BC_RTOL, KNOWN, grid_lines, lines_of
+from util import BC_RTOL, KNOWN, grid_lines, lines_of, unit_grid_lines
 
 pytestmark = pytest.mark.gpu
 
@@ -264,3 +264,19 @@ def test_cli_drop_in(tmp_path):
                        text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     assert "The number of vertices to query: 10" in r.stdout and "vertexID" in r.stdout
+
+
+def test_wrapping_counts_on_device():
+    """32-bit path counts that wrap (unit-weight 24 x 24 grid) are bit-exact on the device, and BC
+    (computed from the wrapped counts, as the reference does) agrees with the oracle"""
+    n, u, v, w = unit_grid_lines()
+    g = _graph(n, u, v, w)
+    for idx in (g.build_index(), g.build_index(on_device=True)):
+        tc = O.TreeCount(n, u, v, w)
+        srcs = np.array([0, 100, n - 1], np.int32)
+        d, c, h = idx.rows(srcs)
+        for k, s in enumerate(srcs):
+            d0, c0, h0 = tc.rows(int(s))
+            assert np.array_equal(d[k], d0) and np.array_equal(c[k], c0) and np.array_equal(h[k], h0)
+        assert int(c[0][-1]) == 4273388464
+        assert rel_err(idx.bc_all(), tc.bc(O.Arcs(n, u, v, w))) <= BC_RTOL

@@ -10,7 +10,7 @@ import gpu_betweennesscentrality_b200 as Q
 import pyoracle as O
 from conftest import GOLDEN, ROOT
 from gpu_betweennesscentrality_b200 import capi, synth
-from util import KNOWN, grid_lines, lines_of
+from util import KNOWN, grid_lines, lines_of, unit_grid_lines
 
 
 def declared_symbols():
@@ -204,3 +204,17 @@ def test_scan_entries_matches_lca_depth_sum():
     want = sum(int(np.minimum(np.cumprod(A == A[tid_of[s]][None, :], axis=1).sum(1), ex["depth"]).sum())
                for s in srcs)
     assert idx.scan_entries(srcs) == want
+
+
+def test_wrapping_counts_unit_grid():
+    """counts beyond 2^32 wrap exactly as the reference's 32-bit arithmetic (uint32 here)"""
+    n, u, v, w = unit_grid_lines()
+    g = Q.Graph()
+    g.ReadLines(n, u, v, w)
+    ex = g.build_index(upload=False).export()
+    arcs = O.Arcs(n, u, v, w)
+    srcs = [0, n // 2 + 5, n - 1]
+    for s, (d, c, h) in zip(srcs, scan_rows(ex, srcs)):
+        d0, c0, h0 = arcs.dijkstra_rows(s)
+        assert np.array_equal(d, d0) and np.array_equal(c, c0) and np.array_equal(h, h0)
+    assert int(arcs.dijkstra_rows(0)[1][-1]) == 4273388464  # C(46, 23) mod 2^32

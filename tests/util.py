@@ -38,3 +38,11 @@ KNOWN = {
                 [(r * 3 + c, (r + 1) * 3 + c, 1) for r in range(2) for c in range(3)], None),
     "path40": (40, [(i, i + 1, 1 + (i % 3)) for i in range(39)], [float(i * (39 - i)) for i in range(40)]),
 }
+
+
+def unit_grid_lines(r=24, c=24):
+    """Unit-weight r x c grid: the shortest-path counts from a corner are binomial coefficients, so
+    at 24 x 24 they exceed 2^32 and the 32-bit count arithmetic wraps (C(46,23) = 8.2e12)."""
+    edges = [(i * c + j, i * c + j + 1, 1) for i in range(r) for j in range(c - 1)]
+    edges += [(i * c + j, (i + 1) * c + j, 1) for i in range(r - 1) for j in range(c)]
+    return lines_of(edges, r * c)
