@@ -570,6 +570,336 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
   if (COUNTS && fin && have && a.maxhop) atomicMax(a.maxhop + first + lane, mh);
 }
 
+// ------------------------------------------------------------------------------- K1 + K2, target pairs
+// Variant of k_label_scan_packed that scans two targets per step: each lane's source-row words
+// are loaded from shared memory once and combined with both target rows, so a step moves 3 instead of
+// 5 shared-memory wavefronts per 128 lane-entries.  Two target rows are scanned while the next two
+// are in flight (4 row buffers per warp), hence 12 warps per CTA to stay within shared memory.
+constexpr int kPairWarps = 12;
+constexpr int kPairBuffers = 4;
+
+__host__ __device__ constexpr size_t pair_smem(int S) {
+  return (size_t)32 * S * 4 + (size_t)kPairWarps * (kPairBuffers * (size_t)S * 4 + kStageInt4 * 16);
+}
+
+// running (min key, min of key ^ mask) over entries [j0, j1) (j1 - j0 a multiple of 8) of one
+// source row and one target row held in shared memory, eight at a time
+__device__ __forceinline__ void scan8(const uint32_t *srow, const int32_t *tbuf, int j0, int j1, uint32_t mask,
+                                      uint32_t &m1, uint32_t &m2) {
+  uint32_t n1 = 0xffffffffu, n2 = 0xffffffffu;
+  for (int j = j0; j < j1; j += 8) {
+    const uint4 x = *reinterpret_cast<const uint4 *>(srow + j);
+    const uint4 y = *reinterpret_cast<const uint4 *>(tbuf + j);
+    const uint4 x2 = *reinterpret_cast<const uint4 *>(srow + j + 4);
+    const uint4 y2 = *reinterpret_cast<const uint4 *>(tbuf + j + 4);
+    const uint32_t v0 = x.x + y.x, v1 = x.y + y.y, v2 = x.z + y.z, v3 = x.w + y.w;
+    const uint32_t u0 = x2.x + y2.x, u1 = x2.y + y2.y, u2 = x2.z + y2.z, u3 = x2.w + y2.w;
+    m1 = __vimin3_u32(m1, v0, v1);
+    n1 = __vimin3_u32(n1, u0, u1);
+    m1 = __vimin3_u32(m1, v2, v3);
+    n1 = __vimin3_u32(n1, u2, u3);
+    m2 = __vimin3_u32(m2, v0 ^ mask, v1 ^ mask);
+    n2 = __vimin3_u32(n2, u0 ^ mask, u1 ^ mask);
+    m2 = __vimin3_u32(m2, v2 ^ mask, v3 ^ mask);
+    n2 = __vimin3_u32(n2, u2 ^ mask, u3 ^ mask);
+  }
+  m1 = min(m1, n1);
+  m2 = min(m2, n2);
+}
+
+// the same over entries [j0, hm) (j0 a multiple of 4), four at a time with the last group masked
+__device__ __forceinline__ void scan_rest(const uint32_t *srow, const int32_t *tbuf, int j0, int hm, uint32_t mask,
+                                          uint32_t &m1, uint32_t &m2) {
+  for (int j = j0; j < hm; j += 4) {
+    const uint4 x = *reinterpret_cast<const uint4 *>(srow + j);
+    const uint4 y = *reinterpret_cast<const uint4 *>(tbuf + j);
+    const uint32_t v0 = x.x + y.x;
+    const uint32_t v1 = (j + 1 < hm) ? x.y + y.y : 0xffffffffu;
+    const uint32_t v2 = (j + 2 < hm) ? x.z + y.z : 0xffffffffu;
+    const uint32_t v3 = (j + 3 < hm) ? x.w + y.w : 0xffffffffu;
+    m1 = __vimin3_u32(m1, v0, v1);
+    m1 = __vimin3_u32(m1, v2, v3);
+    m2 = __vimin3_u32(m2, v0 ^ mask, (j + 1 < hm) ? v1 ^ mask : 0xffffffffu);
+    m2 = __vimin3_u32(m2, (j + 2 < hm) ? v2 ^ mask : 0xffffffffu, (j + 3 < hm) ? v3 ^ mask : 0xffffffffu);
+  }
+}
+
+// the same over entries [S, hl) read from global memory (rows longer than the shared tile)
+__device__ __forceinline__ void scan_global(const int32_t *dis_sh, int64_t soff, int64_t toff, int S, int hl,
+                                            uint32_t mask, uint32_t &m1, uint32_t &m2) {
+  for (int j = S; j < hl; j += 4) {
+    const uint4 x = __ldg(reinterpret_cast<const uint4 *>(dis_sh + soff + j));
+    const uint4 y = __ldg(reinterpret_cast<const uint4 *>(dis_sh + toff + j));
+    const uint32_t v0 = (x.x + y.x) | (uint32_t)j;
+    const uint32_t v1 = (j + 1 < hl) ? ((x.y + y.y) | (uint32_t)(j + 1)) : 0xffffffffu;
+    const uint32_t v2 = (j + 2 < hl) ? ((x.z + y.z) | (uint32_t)(j + 2)) : 0xffffffffu;
+    const uint32_t v3 = (j + 3 < hl) ? ((x.w + y.w) | (uint32_t)(j + 3)) : 0xffffffffu;
+    m1 = __vimin3_u32(m1, v0, v1);
+    m1 = __vimin3_u32(m1, v2, v3);
+    m2 = __vimin3_u32(m2, v0 ^ mask, (j + 1 < hl) ? v1 ^ mask : 0xffffffffu);
+    m2 = __vimin3_u32(m2, (j + 2 < hl) ? v2 ^ mask : 0xffffffffu, (j + 3 < hl) ? v3 ^ mask : 0xffffffffu);
+  }
+}
+
+// distance, and count/hop (or the minimising entry, resolved after the chunk) of one pair from its
+// (m1, m2) keys; ties re-scan the row (shared tile, then global memory)
+template <bool COUNTS>
+__device__ __forceinline__ void finish_pair(const LabelArgs &a, bool have, int k, int t, int hl, uint32_t m1, uint32_t m2,
+                                            uint32_t B, uint32_t mask, const uint32_t *srow, const int32_t *tbuf, int S,
+                                            int64_t soff, int2 *sdc2, int32_t *shp1, uint32_t &pending) {
+  const uint32_t dist = m1 >> B;
+  int cnt = 0, hop = 0;
+  if (COUNTS && have) {
+    if ((m1 ^ m2) == mask) {
+      cnt = (int)(m1 & mask);
+      pending |= 1u << k;
+    } else {
+      const int64_t toff = a.lab_off[t];
+      unsigned cc = 0;
+      int hh = 0;
+      for (int q = 0; q < hl; q++) {
+        const uint32_t dq = q < S ? (srow[q] + (uint32_t)tbuf[q]) >> B
+                                  : ((uint32_t)__ldg(a.dis_sh + soff + q) + (uint32_t)__ldg(a.dis_sh + toff + q)) >> B;
+        if (dq == dist) {
+          const int2 cs = __ldg(a.ch + soff + q), ct = __ldg(a.ch + toff + q);
+          cc += (unsigned)cs.x * (unsigned)ct.x;
+          hh = max(hh, cs.y + ct.y);
+        }
+      }
+      cnt = (int)cc;
+      hop = hh;
+    }
+  }
+  if (have) {
+    sdc2[k] = make_int2((int)dist, cnt);
+    if (COUNTS) shp1[k] = hop;
+  }
+}
+
+template <bool COUNTS>
+__global__ void __launch_bounds__(kPairWarps * 32, 1) k_label_scan_pair(LabelArgs a) {
+  constexpr int G = 32;
+  extern __shared__ int4 smem4[];
+  uint32_t *s_key = reinterpret_cast<uint32_t *>(smem4);
+  const int S = a.stride;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  int32_t *tb0 = reinterpret_cast<int32_t *>(s_key + G * S) + warp * kPairBuffers * S;
+  int4 *sdc = reinterpret_cast<int4 *>(s_key + G * S + nwarps * kPairBuffers * S) + warp * kStageInt4;
+  int4 *shp = sdc + 32 * 5;
+  int2 *sdc2 = reinterpret_cast<int2 *>(sdc) + lane * 10;
+  int32_t *shp1 = reinterpret_cast<int32_t *>(shp) + lane * 12;
+  __shared__ int32_t s_h[G];
+  __shared__ int64_t s_off[G];
+  __shared__ __align__(8) uint64_t s_bar[kPairWarps][kPairBuffers];
+  const int first = blockIdx.y * G;
+  if (first >= a.ns) return;
+  const int gcount = min(G, a.ns - first);
+  const uint32_t B = (uint32_t)a.bits, mask = (1u << B) - 1u;
+  if (threadIdx.x < G) {
+    const int i = threadIdx.x;
+    const int s = i < gcount ? a.src[first + i] : 0;
+    s_h[i] = i < gcount ? a.depth[s] : 0;
+    s_off[i] = a.lab_off[s];
+  }
+  if (lane == 0)
+    for (int b = 0; b < kPairBuffers; b++) mbar_init(&s_bar[warp][b], 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < G * S; idx += blockDim.x) {
+    const int i = idx / S, j = idx - i * S;
+    uint32_t key = 0xffffffffu;
+    if (i < gcount && j < s_h[i]) key = (uint32_t)a.dis_sh[s_off[i] + j] | (uint32_t)j;
+    s_key[idx] = key;
+  }
+  __syncthreads();
+
+  const bool have = lane < gcount;
+  const int hs = have ? s_h[lane] : 1;
+  const int64_t soff = s_off[lane];
+  const uint32_t *srow = s_key + lane * S;
+  const int32_t *lo = a.anc + soff;
+  const int32_t *hi = a.aend + soff;
+  const int nsteps = 32 - __clz(hs);
+  int mh = 0;
+  bool failed = false;
+
+  const int nchunk = a.n_pad >> 3;
+  const int cbeg = (int)((int64_t)nchunk * blockIdx.x / a.split);
+  const int cend = (int)((int64_t)nchunk * (blockIdx.x + 1) / a.split);
+  uint32_t issued = 0, done = 0;
+  int next_c = cbeg + warp, next_k = 0;
+  auto issue_next = [&]() {
+    if (next_c >= cend) return;
+    const int t = next_c * 8 + next_k;
+    if (t >= a.n) { next_c = cend; return; }
+    if (lane == 0) {
+      const uint32_t b = issued % kPairBuffers;
+      const uint32_t bytes = (uint32_t)(min((a.depth[t] + 3) & ~3, S) * 4);  // S is a multiple of 4
+      bulk_row_to_smem(tb0 + b * S, a.dis_sh + a.lab_off[t], bytes, &s_bar[warp][b]);
+    }
+    issued++;
+    if (++next_k == 8) { next_k = 0; next_c += nwarps; }
+  };
+  auto wait_row = [&](const int32_t *&tbuf) {
+    const uint32_t b = done % kPairBuffers;
+    if (!mbar_wait(&s_bar[warp][b], (done / kPairBuffers) & 1)) return false;
+    done++;
+    tbuf = tb0 + b * S;
+    return true;
+  };
+  for (int q = 0; q < kPairBuffers - 2; q++) issue_next();
+
+  for (int c = cbeg + warp; c < cend && !failed; c += nwarps) {
+    const int t0 = c << 3;
+    int J = 0;
+    {
+      int h = have ? hs : 1;
+      for (int it = 0; it < nsteps; it++) {
+        if (h - J > 1) {
+          const int mid = (J + h) >> 1;
+          const bool p = (__ldg(lo + mid) <= t0) && (t0 < __ldg(hi + mid));
+          J = p ? mid : J;
+          h = p ? h : mid;
+        }
+      }
+    }
+    int hiJ = have ? __ldg(hi + J) : 0x7fffffff;
+    int loN = (have && J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
+    // the deepest ancestor interval holding t, moved on from the previous target
+    auto advance = [&](int t) {
+      if (!have) return;
+      if (t >= hiJ) {
+        do { J--; hiJ = __ldg(hi + J); } while (t >= hiJ);
+        loN = __ldg(lo + J + 1);
+      } else if (t == loN) {
+        J++;
+        hiJ = __ldg(hi + J);
+        loN = (J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
+      }
+    };
+    uint32_t pending = 0;
+    const int kend = min(8, a.n - t0);
+    for (int k = 0; k < kend; k += 2) {
+      const int ta = t0 + k, tb = ta + 1;
+      const bool two = k + 1 < kend;
+      if (k > 0) advance(ta);
+      const int hla = have ? J + 1 : 0;
+      int hlb = 0;
+      if (two) {
+        advance(tb);
+        hlb = have ? J + 1 : 0;
+      }
+      issue_next();
+      if (two) issue_next();
+      const int32_t *tba = nullptr, *tbb = nullptr;
+      if (!wait_row(tba) || (two && !wait_row(tbb))) {
+        failed = true;
+        break;
+      }
+      if (!two) tbb = tba;
+      const int hma = min(hla, S), hmb = min(hlb, S);
+      const int full8 = min(hma, hmb) & ~7;
+      uint32_t a1 = 0xffffffffu, a2 = 0xffffffffu, an1 = 0xffffffffu, an2 = 0xffffffffu;
+      uint32_t b1 = 0xffffffffu, b2 = 0xffffffffu, bn1 = 0xffffffffu, bn2 = 0xffffffffu;
+      for (int j = 0; j < full8; j += 8) {  // both targets: one load of the source words
+        const uint4 x = *reinterpret_cast<const uint4 *>(srow + j);
+        const uint4 x2 = *reinterpret_cast<const uint4 *>(srow + j + 4);
+        const uint4 y = *reinterpret_cast<const uint4 *>(tba + j);
+        const uint4 y2 = *reinterpret_cast<const uint4 *>(tba + j + 4);
+        const uint4 z = *reinterpret_cast<const uint4 *>(tbb + j);
+        const uint4 z2 = *reinterpret_cast<const uint4 *>(tbb + j + 4);
+        uint32_t v0 = x.x + y.x, v1 = x.y + y.y, v2 = x.z + y.z, v3 = x.w + y.w;
+        uint32_t u0 = x2.x + y2.x, u1 = x2.y + y2.y, u2 = x2.z + y2.z, u3 = x2.w + y2.w;
+        a1 = __vimin3_u32(a1, v0, v1);
+        an1 = __vimin3_u32(an1, u0, u1);
+        a1 = __vimin3_u32(a1, v2, v3);
+        an1 = __vimin3_u32(an1, u2, u3);
+        a2 = __vimin3_u32(a2, v0 ^ mask, v1 ^ mask);
+        an2 = __vimin3_u32(an2, u0 ^ mask, u1 ^ mask);
+        a2 = __vimin3_u32(a2, v2 ^ mask, v3 ^ mask);
+        an2 = __vimin3_u32(an2, u2 ^ mask, u3 ^ mask);
+        v0 = x.x + z.x, v1 = x.y + z.y, v2 = x.z + z.z, v3 = x.w + z.w;
+        u0 = x2.x + z2.x, u1 = x2.y + z2.y, u2 = x2.z + z2.z, u3 = x2.w + z2.w;
+        b1 = __vimin3_u32(b1, v0, v1);
+        bn1 = __vimin3_u32(bn1, u0, u1);
+        b1 = __vimin3_u32(b1, v2, v3);
+        bn1 = __vimin3_u32(bn1, u2, u3);
+        b2 = __vimin3_u32(b2, v0 ^ mask, v1 ^ mask);
+        bn2 = __vimin3_u32(bn2, u0 ^ mask, u1 ^ mask);
+        b2 = __vimin3_u32(b2, v2 ^ mask, v3 ^ mask);
+        bn2 = __vimin3_u32(bn2, u2 ^ mask, u3 ^ mask);
+      }
+      a1 = min(a1, an1);
+      a2 = min(a2, an2);
+      b1 = min(b1, bn1);
+      b2 = min(b2, bn2);
+      scan8(srow, tba, full8, hma & ~7, mask, a1, a2);
+      scan_rest(srow, tba, hma & ~7, hma, mask, a1, a2);
+      if (hla > S) scan_global(a.dis_sh, soff, a.lab_off[ta], S, hla, mask, a1, a2);
+      finish_pair<COUNTS>(a, have, k, ta, hla, a1, a2, B, mask, srow, tba, S, soff, sdc2, shp1, pending);
+      if (two) {
+        scan8(srow, tbb, full8, hmb & ~7, mask, b1, b2);
+        scan_rest(srow, tbb, hmb & ~7, hmb, mask, b1, b2);
+        if (hlb > S) scan_global(a.dis_sh, soff, a.lab_off[tb], S, hlb, mask, b1, b2);
+        finish_pair<COUNTS>(a, have, k + 1, tb, hlb, b1, b2, B, mask, srow, tbb, S, soff, sdc2, shp1, pending);
+      }
+      __syncwarp();
+    }
+    if (failed) break;
+    if (kend < 8 && have) {
+      for (int k = kend; k < 8; k++) {
+        sdc2[k] = make_int2(0, 0);
+        if (COUNTS) shp1[k] = 0;
+      }
+    }
+    if (COUNTS && have && pending) {
+      int2 cs8[8], ct8[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        if (pending & (1u << k)) {
+          const int jm = sdc2[k].y;
+          cs8[k] = __ldg(a.ch + soff + jm);
+          ct8[k] = __ldg(a.ch + a.lab_off[t0 + k] + jm);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        if (pending & (1u << k)) {
+          sdc2[k].y = (int)((unsigned)cs8[k].x * (unsigned)ct8[k].x);
+          shp1[k] = cs8[k].y + ct8[k].y;
+        }
+      }
+    }
+    if (COUNTS && have) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) mh = max(mh, shp1[k]);
+    }
+    __syncwarp();
+    {
+      int4 *grec = a.out_rec + blk(first, t0, a.ns);
+      const int2 *sdc_all = reinterpret_cast<const int2 *>(sdc);
+      for (int p = lane; p < gcount * 8; p += 32) {
+        const int2 x = sdc_all[(p >> 3) * 10 + (p & 7)];
+        grec[p] = make_int4(x.x, x.y, 0, 0);
+      }
+      if (COUNTS) {
+        int4 *ghp = reinterpret_cast<int4 *>(a.out_hop + blk(first, t0, a.ns));
+        for (int p = lane; p < gcount * 2; p += 32) ghp[p] = shp[(p >> 1) * 3 + (p & 1)];
+      }
+    }
+    __syncwarp();
+  }
+  if (failed) {
+    if (lane == 0 && a.err) atomicCAS(a.err, ERR_NONE, ERR_COPY_TIMEOUT);
+    while (done < issued) {
+      mbar_wait(&s_bar[warp][done % kPairBuffers], (done / kPairBuffers) & 1);
+      done++;
+    }
+    return;
+  }
+  if (COUNTS && have && a.maxhop) atomicMax(a.maxhop + first + lane, mh);
+}
+
 // ------------------------------------------------------------------------------- K3 - K5
 struct DepArgs {
   const int2 *__restrict__ arc_rng;  // per vertex (first arc, end arc)
@@ -1188,14 +1518,16 @@ static int packed_stride(const Handle &h, const DeviceState *d, int warps) {
   const size_t budget = (size_t)std::max(0, d->smem_optin - 2048);
   int S = d->hmax_pad;
   if (h.tuning.label_tile > 0) S = std::min(S, std::max(8, (h.tuning.label_tile + 3) & ~3));
-  while (S > 8 && packed_smem(warps, S) > budget) S -= 4;
+  // warps == 12: the two-target kernel (4 row buffers per warp)
+  auto need = [&](int s) { return warps == 12 ? pair_smem(s) : packed_smem(warps, s); };
+  while (S > 8 && need(S) > budget) S -= 4;
   if (((S / 4) & 1) == 0) S -= 4;
   return S;
 }
 
 // 16 warps when the whole tree height fits, else 8 warps (twice the rows per CTA); or as tuned
 static int packed_warps(const Handle &h, const DeviceState *d) {
-  if (h.tuning.label_warps == 8 || h.tuning.label_warps == 16) return h.tuning.label_warps;
+  if (h.tuning.label_warps == 8 || h.tuning.label_warps == 16 || h.tuning.label_warps == 12) return h.tuning.label_warps;
   return packed_stride(h, d, 16) >= d->hmax_pad ? 16 : 8;
 }
 
@@ -1227,8 +1559,30 @@ static void launch_label_packed_w(const Handle &h, const DeviceState *d, LabelAr
 }
 
 template <bool C>
+static void launch_label_pair(const Handle &h, const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
+  const int S = packed_stride(h, d, 12);
+  const size_t smem = pair_smem(S);
+  const int groups = (ns + 31) / 32;
+  int split = h.tuning.split;
+  if (split <= 0) {
+    split = std::max(1, (148 * 4 + groups - 1) / groups);
+    split = std::min(split, std::max(1, (d->n_pad / 8) / kPairWarps));
+  }
+  a.stride = S;
+  a.split = split;
+  a.multipass = 0;
+  a.pass_lo = 0;
+  CK(cudaFuncSetAttribute(k_label_scan_pair<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(split, groups);
+  k_label_scan_pair<C><<<grid, kPairWarps * 32, smem, st>>>(a);
+  CK(cudaGetLastError());
+}
+
+template <bool C>
 static void launch_label_packed(const Handle &h, const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
-  if (packed_warps(h, d) == 16) launch_label_packed_w<C, 16>(h, d, a, ns, st);
+  const int w = packed_warps(h, d);
+  if (w == 12) launch_label_pair<C>(h, d, a, ns, st);
+  else if (w == 16) launch_label_packed_w<C, 16>(h, d, a, ns, st);
   else launch_label_packed_w<C, 8>(h, d, a, ns, st);
 }
 
