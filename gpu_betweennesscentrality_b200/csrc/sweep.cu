@@ -464,6 +464,7 @@ struct Server {
   std::vector<Req *> active;
   std::map<int64_t, std::unique_ptr<Req>> reqs;
   int64_t next_id = 1;
+  int waiters = 0;  // threads inside serve_wait
   bool stop = false;
   std::string fail;
   std::thread th;
@@ -742,6 +743,15 @@ int serve_wait(Server *s, int64_t ticket, double timeout_s, double *out, double 
   if (it == s->reqs.end()) throw Error(QBC_EINVAL, "unknown ticket " + std::to_string(ticket));
   Req *r = it->second.get();
   auto ready = [&] { return r->state == DONE || r->state == FAILED; };
+  // counted, so that serve_close frees the server only once every waiter has left
+  struct Waiting {
+    Server *s;
+    explicit Waiting(Server *x) : s(x) { s->waiters++; }
+    ~Waiting() {
+      s->waiters--;
+      s->cv_done.notify_all();
+    }
+  } waiting(s);
   if (timeout_s < 0) s->cv_done.wait(lk, ready);
   else s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), ready);
   return take_result(s, it, out, times);
@@ -781,6 +791,11 @@ void serve_close(Server *s) {
   s->cv_work.notify_all();
   s->cv_done.notify_all();
   if (s->th.joinable()) s->th.join();
+  {  // every request is now done or failed: let threads still in serve_wait collect theirs first
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_done.notify_all();
+    s->cv_done.wait(lk, [&] { return s->waiters == 0; });
+  }
   cudaSetDevice(s->d->device);
   cudaStreamSynchronize(s->st);
   if (s->h->server == s) s->h->server = nullptr;

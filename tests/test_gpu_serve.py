@@ -211,3 +211,39 @@ def test_batch_and_serve_on_small_graphs(name):
         ts = [srv.submit(s_) for s_ in sets]
         for s_, t in zip(sets, ts):
             assert np.allclose(srv.wait(t, 60.0)[0], want[s_], rtol=0, atol=1e-9)
+
+
+def test_close_while_clients_wait(g2k):
+    """closing the server fails the requests still queued; threads blocked in wait return with an
+    error instead of hanging, and the index is usable again"""
+    n, idx, full = g2k
+    idx.set_tuning(chunk=64)
+    try:
+        srv = idx.serve(max_active=1)
+        sets = request_sets(n, 30, 500, 500, seed=17)
+        tickets = [srv.submit(s) for s in sets]
+        errors, entered = [], []
+
+        def client(t, ev):
+            ev.set()
+            try:
+                srv.wait(t, 60.0)
+            except Q.QbcError as e:
+                errors.append(e.code)
+
+        for t in tickets[-5:]:
+            ev = threading.Event()
+            th = threading.Thread(target=client, args=(t, ev))
+            th.start()
+            entered.append((th, ev))
+        for th, ev in entered:
+            ev.wait(10.0)
+        time.sleep(0.02)  # the clients are inside the blocking wait call
+        srv.close()
+        for th, _ in entered:
+            th.join(60.0)
+        assert not any(th.is_alive() for th, _ in entered)
+        assert all(code == capi.QBC_EDEVICE for code in errors)
+    finally:
+        idx.set_tuning()
+    assert rel_err(idx.bc_all(), full) <= BC_RTOL
