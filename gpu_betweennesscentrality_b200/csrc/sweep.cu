@@ -434,6 +434,7 @@ struct Req {
   double t_submit = 0, t_admit = 0, t_done = 0;
   std::vector<double> result;
   std::string error;
+  int error_code = QBC_EDEVICE;  // QBC_EBUSY: cancelled by qbc_serve_close
 };
 
 }  // namespace
@@ -714,8 +715,9 @@ static int take_result(Server *s, std::map<int64_t, std::unique_ptr<Req>>::itera
   Req *r = it->second.get();
   if (r->state == FAILED) {
     const std::string msg = r->error;
+    const int code = r->error_code;
     s->reqs.erase(it);
-    throw Error(QBC_EDEVICE, msg);
+    throw Error(code, msg);
   }
   if (r->state != DONE) return 0;
   if (out && !r->result.empty()) std::memcpy(out, r->result.data(), r->result.size() * 8);
@@ -780,11 +782,13 @@ void serve_close(Server *s) {
     for (Req *r : s->queue) {
       r->state = FAILED;
       r->error = "server closed";
+      r->error_code = QBC_EBUSY;
     }
     s->queue.clear();
     for (Req *r : s->active) {
       r->state = FAILED;
       r->error = "server closed";
+      r->error_code = QBC_EBUSY;
     }
     s->active.clear();
   }

@@ -194,7 +194,7 @@ int qbc_serve_wait(qbc_server *srv, int64_t ticket, double timeout_s, double *ou
 /* out[0]=chunks run, [1]=turns over the sources, [2]=requests done, [3]=active, [4]=queued,
  * [5]=pool entries in use, [6]=pool capacity, [7]=chunks per turn, [8]=sources per turn */
 int qbc_serve_stats(qbc_server *srv, double *out, int32_t nout);
-/* cancels queued and active requests (their waiters get an error), waits for the device work in
+/* cancels queued and active requests (their waiters get QBC_EBUSY), waits for the device work in
  * flight and for threads still inside qbc_serve_wait to return, then frees the server; no call on
  * the server may start once qbc_serve_close has been called */
 int qbc_serve_close(qbc_server *srv);
