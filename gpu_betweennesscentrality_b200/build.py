@@ -69,14 +69,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if not force and not _stale(o, [s] + headers + [__file__]):
             continue
         if kind == "cxx":
-            cmd = [cxx, "-O3", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function", "-pthread",
+            cmd = [cxx, "-O3", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function", "-pthread", "-fopenmp",
                    "-I", INCLUDE, "-c", s, "-o", o]
         else:
             cmd = [nvcc, "-O3", "-std=c++17", *GENCODE, "-lineinfo", "-ccbin", cxx, "-Xcompiler", "-fPIC",
                    "-I", INCLUDE, "-c", s, "-o", o]
         _run(cmd, verbose)
     if force or _stale(LIB, objs):
-        _run([nvcc, "-shared", *GENCODE, "-ccbin", cxx, "-o", LIB, *objs, "-lpthread"], verbose)
+        _run([nvcc, "-shared", *GENCODE, "-ccbin", cxx, "-o", LIB, *objs, "-lpthread", "-lgomp"], verbose)
     cli_src = os.path.join(CSRC, "cli.cpp")
     for name, macro in CLIS.items():
         out = os.path.join(BIN, name)

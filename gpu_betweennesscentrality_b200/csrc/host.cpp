@@ -17,7 +17,12 @@
 #include <queue>
 #include <thread>
 
+#include <omp.h>
+
 namespace qbc {
+
+// separators at least this large are merged into their neighbours' lists in parallel
+constexpr int32_t kParallelSeparator = 192;
 
 int hardware_threads(int requested) {
   if (requested > 0) return requested;
@@ -228,6 +233,8 @@ struct Elimination {
 
 Elimination eliminate(const Graph &g, const std::vector<int32_t> *fixed_order) {
   const int32_t n = g.n;
+  const int nthreads = hardware_threads(0);
+  std::vector<std::vector<int32_t>> stamp_t, where_t;  // per-thread stamps for large separators
   std::vector<std::vector<Adj>> adj((size_t)n);
   for (int32_t a = 0; a < n; a++)
     for (int32_t e = g.off[a]; e < g.off[a + 1]; e++) adj[a].push_back({g.head[e], g.w[e], 1u, 1});
@@ -269,34 +276,50 @@ Elimination eliminate(const Graph &g, const std::vector<int32_t> *fixed_order) {
     adj[x].shrink_to_fit();
     const int32_t k = (int32_t)X.size();
     el.width = std::max(el.width, k);
-    for (int32_t i = 0; i < k; i++) {
+    // Neighbour u of x gets the shortcuts through x to every other neighbour.  stamp/where mark u's
+    // current neighbours; a stale stamp (v marked for u earlier, v no longer in u's list) can only
+    // belong to an eliminated v, which never reappears in a separator, so stamps are not cleared.
+    auto merge = [&](int32_t i, std::vector<int32_t> &stp, std::vector<int32_t> &whr) {
       const int32_t u = X[i].v;
       std::vector<Adj> &au = adj[u];
       // drop x from u
       for (size_t e = 0; e < au.size(); e++)
         if (au[e].v == x) { au[e] = au.back(); au.pop_back(); break; }
-      for (size_t e = 0; e < au.size(); e++) { stamp[au[e].v] = u; where[au[e].v] = (int32_t)e; }
+      for (size_t e = 0; e < au.size(); e++) { stp[au[e].v] = u; whr[au[e].v] = (int32_t)e; }
       for (int32_t j = 0; j < k; j++) {
         if (j == i) continue;
         const int32_t v = X[j].v;
         const int32_t nl = X[i].len + X[j].len;
         const uint32_t nc = X[i].cnt * X[j].cnt;
         const int32_t nh = X[i].hop + X[j].hop;
-        if (stamp[v] == u) {
-          Adj &a = au[where[v]];
+        if (stp[v] == u) {
+          Adj &a = au[whr[v]];
           if (nl < a.len) { a.len = nl; a.cnt = nc; a.hop = nh; }
           else if (nl == a.len) { a.cnt += nc; if (nh > a.hop) a.hop = nh; }
         } else {
-          stamp[v] = u;
-          where[v] = (int32_t)au.size();
+          stp[v] = u;
+          whr[v] = (int32_t)au.size();
           au.push_back({v, nl, nc, nh});
         }
       }
+    };
+    if (k >= kParallelSeparator && nthreads > 1) {
+      // the large separators near the top of the tree dominate the elimination: their neighbours'
+      // lists are updated in parallel (each neighbour by one thread, with its own stamp arrays)
+      if (stamp_t.empty()) {
+        stamp_t.assign((size_t)nthreads, std::vector<int32_t>((size_t)n, -1));
+        where_t.assign((size_t)nthreads, std::vector<int32_t>((size_t)n, 0));
+      }
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
+      for (int32_t i = 0; i < k; i++) {
+        const int t = omp_get_thread_num();
+        merge(i, stamp_t[t], where_t[t]);
+      }
+    } else {
+      for (int32_t i = 0; i < k; i++) merge(i, stamp, where);
     }
-    for (int32_t i = 0; i < k; i++) {
-      stamp[X[i].v] = -1;
-      if (!fixed_order) pq.push({(int64_t)adj[X[i].v].size(), X[i].v});
-    }
+    if (!fixed_order)
+      for (int32_t i = 0; i < k; i++) pq.push({(int64_t)adj[X[i].v].size(), X[i].v});
     // any stamps left by neighbours-of-neighbours are harmless: they compare against a vertex id
     el.x.insert(el.x.end(), X.begin(), X.end());
     el.x_off.push_back((int64_t)el.x.size());

@@ -131,8 +131,10 @@ def scan_rows(ex, sources_vid):
     return out
 
 
-@pytest.mark.parametrize("n_target,seed,sc", [(2000, 1, 0.0), (900, 5, 0.02), (300, 8, 0.05)])
+@pytest.mark.parametrize("n_target,seed,sc", [(2000, 1, 0.0), (900, 5, 0.02), (300, 8, 0.05), (6000, 11, 0.05)])
 def test_mhl_index_rows_match_oracle(n_target, seed, sc):
+    """the last case has separators of more than 192 vertices, which the elimination merges into
+    their neighbours' lists in parallel"""
     n, u, v, w = grid_lines(n_target, seed=seed, shortcut_frac=sc)
     g = Q.Graph(nthreads=4)
     g.ReadLines(n, u, v, w)
