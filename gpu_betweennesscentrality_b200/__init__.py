@@ -293,12 +293,12 @@ class Graph:
 
     def brandesBCIndexGPU_5(self, roadName: str, orderFile: Optional[str] = None) -> None:
         if orderFile is None:
-            idx = self.build_index(QBC_INDEX_MHL)
+            idx = self.build_index(QBC_INDEX_MHL, on_device=True)
         else:
-            idx = self.build_index(QBC_INDEX_H2H, read_order(orderFile, self.nodenum))
+            idx = self.build_index(QBC_INDEX_H2H, read_order(orderFile, self.nodenum), on_device=True)
         self.BC = idx.bc_all()
 
     def brandesBCIndexGPU_PointBatch(self, roadName: str, points, querySize: int) -> None:
         pts = i32(points)[:querySize]
-        idx = self.build_index(QBC_INDEX_MHL)
+        idx = self.build_index(QBC_INDEX_MHL, on_device=True)
         self.h_PointBC = idx.bc_query(pts)

@@ -80,8 +80,8 @@ class Graph {
   void build(int kind, const int32_t *order) {
     if (!g_) throw std::runtime_error("qbc: ReadGraph first");
     if (idx_) { qbc_index_free(idx_); idx_ = nullptr; }
-    check(qbc_index_build(g_, kind, order, nthreads, &idx_));
-    check(qbc_index_upload(idx_, device));
+    // elimination on the host, label rows filled on the GPU (qbc_index_build_device)
+    check(qbc_index_build_device(g_, kind, order, device, &idx_));
   }
 };
 
