@@ -27,7 +27,7 @@ class Graph {
   int nodenum = 0;
   int edgenum = 0;          // arcs kept by the reader
   int device = 0;           // cudaSetDevice target (QBC.cu:601-602)
-  int nthreads = 0;         // host threads of the index build (0 = all)
+  int nthreads = 0;         // kept for source compatibility; the elimination uses all host threads
   std::vector<double> BC;         // include/Graph.h:71
   std::vector<double> h_PointBC;  // include/Graph.h:198
 
