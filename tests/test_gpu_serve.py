@@ -247,3 +247,23 @@ def test_close_while_clients_wait(g2k):
     finally:
         idx.set_tuning()
     assert rel_err(idx.bc_all(), full) <= BC_RTOL
+
+
+def test_la_query_batch_and_served_match_reference_gpu(la_path, la_query_path):
+    """the reference's own query batch on its LosAngeles graph: batched and served RQ equal the
+    reference GPU's BC of those vertices (RQ = BC restricted to the set)"""
+    p = os.path.join(GOLDEN, "ref_la_mhl.npz")
+    if not os.path.exists(p):
+        pytest.skip("ref_la_mhl.npz not generated")
+    ref = np.load(p)["bc"]
+    g = Q.Graph(device=0)
+    g.ReadGraph(la_path)
+    idx = g.build_index(on_device=True)
+    q = Q.read_query(la_query_path, g.nodenum)
+    sets = [q, q[::-1], q[:3]]
+    for s_, o in zip(sets, idx.bc_query_batch(sets)):
+        assert rel_err(o, ref[s_]) <= BC_RTOL
+    with idx.serve() as srv:
+        ts = [srv.submit(s_) for s_ in sets]
+        for s_, t in zip(sets, ts):
+            assert rel_err(srv.wait(t, 120.0)[0], ref[s_]) <= BC_RTOL
