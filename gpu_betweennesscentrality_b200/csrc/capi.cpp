@@ -254,8 +254,8 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
     if (nparams > 5) need(params[5] >= 0 && params[5] <= 4, "dependency form must be 0..4");
     if (nparams > 6) need(params[6] == 0 || (params[6] >= 64 && params[6] <= 2048), "queue depth must be 0 or in [64, 2048]");
     if (nparams > 7)
-      need(params[7] == 0 || params[7] == 8 || params[7] == 12 || params[7] == 16,
-           "label warps must be 0, 8, 12 (two-target kernel) or 16");
+      need(params[7] == 0 || params[7] == 8 || params[7] == 12 || params[7] == 16 || params[7] == 20,
+           "label warps must be 0, 8, 12 (two-target kernel), 16 or 20");
     if (nparams > 8) need(params[8] >= 0, "label tile must be >= 0");
     if (nparams > 9) need(params[9] >= 0 && params[9] <= 2, "label passes must be 0, 1 or 2");
     for (int32_t i = 0; i < nparams && i < 10; i++) *f[i] = params[i];

@@ -1525,9 +1525,11 @@ static int packed_stride(const Handle &h, const DeviceState *d, int warps) {
   return S;
 }
 
-// 16 warps when the whole tree height fits, else 8 warps (twice the rows per CTA); or as tuned
+// 20 (or 16) warps when the whole tree height fits, else 8 warps (twice the rows per CTA); or as tuned
 static int packed_warps(const Handle &h, const DeviceState *d) {
-  if (h.tuning.label_warps == 8 || h.tuning.label_warps == 16 || h.tuning.label_warps == 12) return h.tuning.label_warps;
+  const int w = h.tuning.label_warps;
+  if (w == 8 || w == 12 || w == 16 || w == 20) return w;
+  if (packed_stride(h, d, 20) >= d->hmax_pad) return 20;  // 96 registers/thread: 20 warps fit
   return packed_stride(h, d, 16) >= d->hmax_pad ? 16 : 8;
 }
 
@@ -1583,6 +1585,7 @@ static void launch_label_packed(const Handle &h, const DeviceState *d, LabelArgs
   const int w = packed_warps(h, d);
   if (w == 12) launch_label_pair<C>(h, d, a, ns, st);
   else if (w == 16) launch_label_packed_w<C, 16>(h, d, a, ns, st);
+  else if (w == 20) launch_label_packed_w<C, 20>(h, d, a, ns, st);
   else launch_label_packed_w<C, 8>(h, d, a, ns, st);
 }
 

@@ -17,7 +17,7 @@ struct Tuning {
   int32_t dep_form = 0;          // 0 auto (= 3 for MHL), 1 warp per source, 2 CTA per source, 3 warp per
                                  // source with a software-pipelined backprop, 4 CTA per source, pipelined
   int32_t queue_depth = 0;       // level-queue layers held in shared memory by the warp form; 0 = 512
-  int32_t label_warps = 0;       // packed-key label kernel: 8 or 16 warps, 12 = two-target kernel; 0 = auto
+  int32_t label_warps = 0;       // packed-key label kernel: 8, 16 or 20 warps, 12 = two-target kernel; 0 = auto
   int32_t label_tile = 0;        // label entries per row staged in shared memory; 0 = all that fit
   int32_t label_passes = 0;      // rows longer than the tile: 0/1 one pass + global tail, 2 several tile passes
 };

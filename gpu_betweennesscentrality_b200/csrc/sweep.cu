@@ -328,7 +328,7 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
     //    passes or a global-memory tail, or the general kernel
     //    with 32/K sources per CTA and 128 or 256 threads
     if (d->packed_bits)
-      for (int32_t warps : {8, 12, 16})  // 12: the two-target kernel
+      for (int32_t warps : {8, 12, 16, 20})  // 12: the two-target kernel
         for (int32_t passes : {0, 2}) {  // rows taller than a 16-warp tile: global tail or tile passes
           if (passes == 2 && (d->hmax_pad <= 644 || warps == 12)) continue;
           Tuning t = best;

@@ -106,7 +106,7 @@ int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int3
  * layer-independent loads issued one to three steps ahead, 4 one CTA per source, pipelined the
  * same way), [6]=level-queue depth of the warp form (layers
  * counted in shared memory, 64..2048; 0 = 512), [7]=warps per CTA of the packed-key kernel (8 or
- * 16; 0 = 16 when the whole tree height fits shared memory, else 8; 12 = a 12-warp kernel that scans
+ * 16 or 20; 0 = the most warps whose shared memory holds the whole tree height, else 8; 12 = a 12-warp kernel that scans
  * two targets per step against one load of the source words), [8]=label tile: entries of
  * each row staged in shared memory by the packed-key kernel (0 = all that fit; later entries of a
  * scan are read from global memory or taken in further passes, see [9]), [9]=label passes for

@@ -61,7 +61,8 @@ def test_rows_identical_across_tunings(g2k, lanes):
 
 @pytest.mark.parametrize("warps,tile,passes", [(16, 0, 0), (8, 0, 0), (16, 32, 1), (8, 48, 1), (16, 8, 1),
                                                (16, 32, 2), (8, 48, 2), (16, 8, 2), (8, 20, 0),
-                                               (12, 0, 0), (12, 32, 0), (12, 8, 0), (12, 44, 0)])
+                                               (12, 0, 0), (12, 32, 0), (12, 8, 0), (12, 44, 0),
+                                               (20, 0, 0), (20, 40, 0), (20, 40, 2)])
 def test_packed_kernel_tiles_and_warps(g2k, warps, tile, passes):
     """rows longer than the shared-memory tile: several tile passes (state kept in the output rows)
     or one pass with the entries beyond the tile from global memory: same rows, same BC"""
