@@ -1257,7 +1257,7 @@ __global__ void __launch_bounds__(256, 3) k_dependency_warp(DepArgs a, const int
 // CTA-per-source form with the software-pipelined backprop of k_dependency_warp<true> (steps of
 // blockDim.x vertices, a __syncthreads between layers); the largest layer comes from the label
 // kernel, so the pass over the hop layers that k_dependency makes to find it is skipped.
-__global__ void __launch_bounds__(256, 4) k_dependency_cta_pipe(DepArgs a, const int32_t *__restrict__ maxhop) {
+__global__ void __launch_bounds__(256, 3) k_dependency_cta_pipe(DepArgs a, const int32_t *__restrict__ maxhop) {
   __shared__ int sh_cnt[kLayerCap + 2];
   __shared__ int sh_cur[kLayerCap + 2];
   __shared__ int red[33];
