@@ -1665,7 +1665,10 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *
                        bool plain = false) {
   DepArgs a = dep_args(d, buf, src, ns);
   const int threads = std::max(64, std::min(256, (h.tuning.dep_threads / 32) * 32));
-  const bool warp_form = h.host.kind == IndexKind::MHL && h.tuning.dep_form != 2 && h.tuning.dep_form != 4 && !plain;
+  // auto (0) = the CTA-per-source pipelined pass: measured fastest at 50k (108 ms per step vs 153
+  // for the pipelined warp form and 151 for the plain CTA form)
+  const int form = h.tuning.dep_form == 0 ? 4 : h.tuning.dep_form;
+  const bool warp_form = h.host.kind == IndexKind::MHL && (form == 1 || form == 3) && !plain;
   std::pair<cudaEvent_t, cudaEvent_t> ev{};
   if (d->profiling) {
     ev = take_events(d->ev_dp, d->ev_dp_used);
@@ -1679,11 +1682,10 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *
       CK(cudaFuncSetAttribute(k_dependency_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       CK(cudaFuncSetAttribute(k_dependency_warp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
-    // auto (0) = the software-pipelined backprop: measured fastest at 50k (162 vs 176-191 ms)
-    if (h.tuning.dep_form == 3 || h.tuning.dep_form == 0)
+    if (form == 3)
       k_dependency_warp<true><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
     else k_dependency_warp<false><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
-  } else if (h.host.kind == IndexKind::MHL && h.tuning.dep_form == 4) {
+  } else if (h.host.kind == IndexKind::MHL && form == 4 && !plain) {
     k_dependency_cta_pipe<<<ns, threads, 0, st>>>(a, d->maxhop[buf]);
   } else if (h.host.kind == IndexKind::MHL) {
     k_dependency<<<ns, threads, 0, st>>>(a);

@@ -14,7 +14,7 @@ struct Tuning {
   int32_t split = 0;             // target ranges per source group; 0 = auto
   int32_t chunk = 0;             // sources per scratch buffer; 0 = auto
   int32_t dep_threads = 256;     // threads per CTA of the CTA-per-source dependency kernel
-  int32_t dep_form = 0;          // 0 auto (= 3 for MHL), 1 warp per source, 2 CTA per source, 3 warp per
+  int32_t dep_form = 0;          // 0 auto (= 4 for MHL), 1 warp per source, 2 CTA per source, 3 warp per
                                  // source with a software-pipelined backprop, 4 CTA per source, pipelined
   int32_t queue_depth = 0;       // level-queue layers held in shared memory by the warp form; 0 = 512
   int32_t label_warps = 0;       // packed-key label kernel: 8, 16 or 20 warps, 12 = two-target kernel; 0 = auto

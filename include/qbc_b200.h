@@ -101,7 +101,7 @@ int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int3
  * packed-key kernel when the index allows it, else the smallest K whose rows fit shared memory;
  * 1..32 forces the general kernel with 32/K sources per CTA), [1]=threads per CTA of the general
  * label kernel, [2]=target split per source group (0=auto), [3]=sources per chunk (0=auto),
- * [4]=threads per CTA of the CTA-per-source dependency kernel, [5]=dependency form (0 auto = 3,
+ * [4]=threads per CTA of the CTA-per-source dependency kernel, [5]=dependency form (0 auto = 4,
  * 1 one warp per source, 2 one CTA per source, 3 one warp per source with the backprop's
  * layer-independent loads issued one to three steps ahead, 4 one CTA per source, pipelined the
  * same way), [6]=level-queue depth of the warp form (layers
