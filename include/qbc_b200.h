@@ -28,8 +28,9 @@ enum {
   QBC_ECUDA = 4,    /* CUDA runtime error */
   QBC_ENOMEM = 5,   /* device or host allocation refused */
   QBC_EDEVICE = 6,  /* a kernel reported an error word (capacity exceeded, bound hit) */
-  QBC_ETIMEOUT = 7, /* served-mode wait ran out */
-  QBC_EBUSY = 8     /* served-mode admission refused (no slot / not enough free HBM) */
+  QBC_ETIMEOUT = 7, /* reserved (a served wait that runs out returns QBC_OK with *done = 0) */
+  QBC_EBUSY = 8     /* the index is serving, the request queue is full, or a request was
+                       cancelled by qbc_serve_close */
 };
 
 enum {
