@@ -1842,6 +1842,79 @@ __global__ void __launch_bounds__(256) k_fill_level(FillArgs f, const int32_t *_
   }
 }
 
+// The same fill for nodes with large separators (near the root): one CTA per node, the separator
+// entries with their vertices' row offsets and depths staged in shared memory, threads over the
+// row's entries.  A warp per node there spends its time on dependent per-separator loads.
+constexpr int kBigSeparator = 32;  // separators of at least this size take the CTA form
+constexpr int kFillStageBytes = 28;  // shared bytes per staged separator entry
+
+template <bool MHL>
+__global__ void __launch_bounds__(256) k_fill_node_cta(FillArgs f, const int32_t *__restrict__ nodes) {
+  extern __shared__ int4 fsm[];
+  const int p = nodes[blockIdx.x];
+  const int h = f.depth[p];
+  const int64_t off = f.lab_off[p];
+  const int par = f.parent[p];
+  const int64_t poff = par >= 0 ? f.lab_off[par] : 0;
+  const int64_t sb = f.sep_off[p];
+  const int nx = (int)(f.sep_off[p + 1] - sb);
+  int4 *s_sep = fsm;
+  int64_t *s_xoff = reinterpret_cast<int64_t *>(s_sep + nx);
+  int32_t *s_k = reinterpret_cast<int32_t *>(s_xoff + nx);
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    const int4 x = f.sep[sb + i];
+    s_sep[i] = x;
+    s_xoff[i] = f.lab_off[x.x];
+    s_k[i] = f.depth[x.x] - 1;
+  }
+  for (int j = threadIdx.x; j < h; j += blockDim.x) {  // ancestor row: the parent's plus p itself
+    const int a = (j < h - 1) ? f.anc[poff + j] : p;
+    f.anc[off + j] = a;
+    f.aend[off + j] = f.send[a];
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < h - 1; j += blockDim.x) {
+    int best = kInfDist;
+    unsigned c = 0;
+    int hp = 0;
+    const int64_t ajoff = MHL ? 0 : f.lab_off[f.anc[off + j]];
+    for (int i = 0; i < nx; i++) {
+      const int4 x = s_sep[i];
+      const int k = s_k[i];
+      int nd;
+      unsigned nc = 0;
+      int nh = 0;
+      if (j <= k) {
+        const int64_t xo = s_xoff[i] + j;
+        nd = x.y + f.dis[xo];
+        if (MHL) {
+          const int2 cx = f.ch[xo];
+          nc = (unsigned)x.z * (unsigned)cx.x;
+          nh = x.w + cx.y;
+        }
+      } else if (!MHL) {
+        nd = x.y + f.dis[ajoff + k];
+      } else {
+        continue;
+      }
+      if (nd < best) {
+        best = nd;
+        c = nc;
+        hp = nh;
+      } else if (MHL && nd == best) {
+        c += nc;
+        hp = max(hp, nh);
+      }
+    }
+    f.dis[off + j] = best;
+    if (MHL) f.ch[off + j] = make_int2((int)c, hp);
+  }
+  if (threadIdx.x == 0) {
+    f.dis[off + h - 1] = 0;
+    if (MHL) f.ch[off + h - 1] = make_int2(1, 0);
+  }
+}
+
 __global__ void k_shift_left(const int32_t *__restrict__ in, int32_t *__restrict__ out, int64_t n, int bits) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     out[i] = (int32_t)((uint32_t)in[i] << bits);
@@ -1960,14 +2033,32 @@ void device_build(Handle &h, int device, const Separators &seps) {
       d->ch = dmalloc<int2>(d, (size_t)L);
       CK(cudaMemsetAsync(d->ch, 0, (size_t)L * 8, st));
     }
-    // nodes grouped by depth (counting sort; preorder keeps each level in increasing tid order)
-    std::vector<int64_t> lvl((size_t)ix.tree_height + 2, 0);
-    for (int32_t t = 0; t < ix.n; t++) lvl[ix.depth[t] + 1]++;
+    // nodes grouped by depth (counting sort; preorder keeps each level in increasing tid order);
+    // within a level, nodes with small separators first (warp per node), then large ones (CTA per
+    // node, separators staged in shared memory; beyond the staging capacity they stay warp-filled)
+    const int64_t stage_cap = std::max(kBigSeparator, (d->smem_optin - 1024) / kFillStageBytes);
+    auto big = [&](int32_t t) {
+      const int64_t nx = seps.off[t + 1] - seps.off[t];
+      return nx >= kBigSeparator && nx <= stage_cap;
+    };
+    std::vector<int64_t> lvl((size_t)ix.tree_height + 2, 0), nbig((size_t)ix.tree_height + 2, 0),
+        maxsep((size_t)ix.tree_height + 2, 0);
+    for (int32_t t = 0; t < ix.n; t++) {
+      lvl[ix.depth[t] + 1]++;
+      if (big(t)) {
+        nbig[ix.depth[t]]++;
+        maxsep[ix.depth[t]] = std::max(maxsep[ix.depth[t]], seps.off[t + 1] - seps.off[t]);
+      }
+    }
     for (size_t k = 1; k < lvl.size(); k++) lvl[k] += lvl[k - 1];
     std::vector<int32_t> nodes((size_t)ix.n);
     {
-      std::vector<int64_t> fillp(lvl.begin(), lvl.end() - 1);
-      for (int32_t t = 0; t < ix.n; t++) nodes[fillp[ix.depth[t]]++] = t;
+      std::vector<int64_t> fs(lvl.begin(), lvl.end() - 1), fb((size_t)ix.tree_height + 2, 0);
+      for (size_t k = 0; k + 1 < lvl.size(); k++) fb[k] = lvl[k + 1] - nbig[k];
+      for (int32_t t = 0; t < ix.n; t++) {
+        if (big(t)) nodes[fb[ix.depth[t]]++] = t;
+        else nodes[fs[ix.depth[t]]++] = t;
+      }
     }
     // temporaries of the fill, freed at the end
     int32_t *d_nodes = nullptr, *d_parent = nullptr, *d_max = nullptr;
@@ -1990,13 +2081,23 @@ void device_build(Handle &h, int device, const Separators &seps) {
       if (!seps.ent.empty()) CK(cudaMemcpyAsync(d_sep, seps.ent.data(), seps.ent.size() * 4, cudaMemcpyHostToDevice, st));
       CK(cudaMemsetAsync(d_max, 0, 4, st));
       FillArgs f{d->depth, d_parent, d->send, d->lab_off, d_soff, d_sep, d->dis, d->ch, d->anc, d->aend};
+      const size_t max_stage = (size_t)stage_cap * kFillStageBytes;
+      CK(cudaFuncSetAttribute(k_fill_node_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_stage));
+      CK(cudaFuncSetAttribute(k_fill_node_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_stage));
       for (int32_t k = 1; k <= ix.tree_height; k++) {
-        const int count = (int)(lvl[k + 1] - lvl[k]);
-        if (count == 0) continue;
-        const int blocks = (count + 7) / 8;
-        if (mhl) k_fill_level<true><<<blocks, 256, 0, st>>>(f, d_nodes + lvl[k], count);
-        else k_fill_level<false><<<blocks, 256, 0, st>>>(f, d_nodes + lvl[k], count);
-        CK(cudaGetLastError());
+        const int count = (int)(lvl[k + 1] - lvl[k] - nbig[k]);
+        if (count > 0) {
+          const int blocks = (count + 7) / 8;
+          if (mhl) k_fill_level<true><<<blocks, 256, 0, st>>>(f, d_nodes + lvl[k], count);
+          else k_fill_level<false><<<blocks, 256, 0, st>>>(f, d_nodes + lvl[k], count);
+          CK(cudaGetLastError());
+        }
+        if (nbig[k] > 0) {
+          const size_t smem = (size_t)maxsep[k] * kFillStageBytes;
+          if (mhl) k_fill_node_cta<true><<<(unsigned)nbig[k], 256, smem, st>>>(f, d_nodes + lvl[k + 1] - nbig[k]);
+          else k_fill_node_cta<false><<<(unsigned)nbig[k], 256, smem, st>>>(f, d_nodes + lvl[k + 1] - nbig[k]);
+          CK(cudaGetLastError());
+        }
       }
       k_max_i32<<<148 * 4, 256, 0, st>>>(d->dis, L, d_max);
       CK(cudaGetLastError());
