@@ -209,6 +209,32 @@ def test_50k_sampled_rows_and_partial_bc(graph_cache):
     assert rel_err(idx.bc_sources(srcs), tc.bc(O.Arcs(n, u, v, w), srcs)) <= BC_RTOL
 
 
+def test_200k_tall_tree_rows_and_partial_bc(graph_cache):
+    """the 200k grid's tree (height 1,088) is taller than the label kernel's shared tile: entries
+    beyond it come from global memory (default), from further tile passes, or with 16 warps from a
+    longer global tail -- rows bit-exact and partial BC against the oracle in every case"""
+    path = synth.cached_graph(graph_cache, 200000, seed=1)
+    n, u, v, w = synth.read_graph_lines(path)
+    g = Q.Graph(device=0)
+    g.ReadGraph(path)
+    idx = g.build_index(on_device=True)
+    assert idx.info()[3] > 1024
+    tc = O.TreeCount(n, u, v, w)
+    rng = np.random.default_rng(22)
+    srcs = np.sort(rng.choice(n, 16, replace=False)).astype(np.int32)
+    want = [tc.rows(int(s)) for s in srcs[:4]]
+    try:
+        for tune in ({}, {"label_warps": 16}, {"label_passes": 2}, {"label_warps": 12}):
+            idx.set_tuning(**tune)
+            d, c, h = idx.rows(srcs[:4])
+            for k in range(4):
+                d0, c0, h0 = want[k]
+                assert np.array_equal(d[k], d0) and np.array_equal(c[k], c0) and np.array_equal(h[k], h0), tune
+    finally:
+        idx.set_tuning()
+    assert rel_err(idx.bc_sources(srcs), tc.bc(O.Arcs(n, u, v, w), srcs)) <= BC_RTOL
+
+
 def test_la_full_bc_matches_reference_gpu(la_path):
     p = os.path.join(GOLDEN, "ref_la_mhl.npz")
     g = Q.Graph(device=0)
