@@ -905,6 +905,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 1) k_label_scan_pair(LabelArg
 struct DepArgs {
   const int2 *__restrict__ arc_rng;  // per vertex (first arc, end arc)
   const int2 *__restrict__ arc_hw;   // per arc (head, weight)
+  const int4 *__restrict__ arc4;     // per vertex its first four arcs in 32 bytes (arc4_of)
   const int32_t *__restrict__ arc_off;
   const int32_t *__restrict__ arc_head;
   const int32_t *__restrict__ arc_w;
@@ -1309,44 +1310,43 @@ __device__ __forceinline__ void dep_cta_pipe_body(const DepArgs &a, int slot, in
   }
   __syncthreads();
   const CNT *start = cnt - 1;  // layer L is [start[L], start[L + 1]) for L >= 1
+  // Pipeline over steps: the queue entry of a step is loaded three steps before it is computed,
+  // its own record two, its arcs one; a step then waits only for its successors' records (rho
+  // written by the layer before).
   StepIt itC = step_first(start, maxL);
   StepIt itB = step_next(start, itC, W);
   StepIt itA = step_next(start, itB, W);
   auto vertex_at = [&](const StepIt &it) {
     return (it.L >= 1 && it.idx + tid < it.end) ? __ldcg(order + it.idx + tid) : -1;
   };
-  auto arc_at = [&](int e, int end) { return e < end ? __ldcg(a.arc_hw + e) : make_int2(-1, 0); };
+  const int4 none = make_int4(-1, 0, -1, 0);
   int vC = vertex_at(itC);
   int4 rC = vC >= 0 ? rec[vC] : make_int4(0, 0, 0, 0);
-  int2 gC = vC >= 0 ? __ldcg(a.arc_rng + vC) : make_int2(0, 0);
-  int2 hC[4];
-#pragma unroll
-  for (int q = 0; q < 4; q++) hC[q] = arc_at(gC.x + q, gC.y);
+  int4 aC0 = vC >= 0 ? __ldcg(a.arc4 + 2 * vC) : none, aC1 = vC >= 0 ? __ldcg(a.arc4 + 2 * vC + 1) : none;
   int vB = vertex_at(itB);
   int4 rB = vB >= 0 ? rec[vB] : make_int4(0, 0, 0, 0);
-  int2 gB = vB >= 0 ? __ldcg(a.arc_rng + vB) : make_int2(0, 0);
   int vA = vertex_at(itA);
   while (itC.L >= 1) {
-    int2 hB[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) hB[q] = arc_at(gB.x + q, gB.y);
+    const int4 aB0 = vB >= 0 ? __ldcg(a.arc4 + 2 * vB) : none, aB1 = vB >= 0 ? __ldcg(a.arc4 + 2 * vB + 1) : none;
     const int4 rA = vA >= 0 ? rec[vA] : make_int4(0, 0, 0, 0);
-    const int2 gA = vA >= 0 ? __ldcg(a.arc_rng + vA) : make_int2(0, 0);
     const StepIt itN = step_next(start, itA, W);
     const int vN = vertex_at(itN);
     if (vC >= 0) {
+      const int hd[4] = {aC0.x, aC0.z, aC1.x, aC1.z}, wt[4] = {aC0.y, aC0.w, aC1.y, aC1.w};
       int4 rw[4];
 #pragma unroll
       for (int q = 0; q < 4; q++)
-        if (hC[q].x >= 0) rw[q] = rec[hC[q].x];
+        if (hd[q] >= 0) rw[q] = rec[hd[q]];
       double acc = 0.0;
 #pragma unroll
       for (int q = 0; q < 4; q++)
-        if (hC[q].x >= 0 && rw[q].x == rC.x + hC[q].y) acc += rec_rho(rw[q]);
-      for (int e = gC.x + 4; e < gC.y; e++) {
-        const int2 hw = __ldcg(a.arc_hw + e);
-        const int4 r = rec[hw.x];
-        if (r.x == rC.x + hw.y) acc += rec_rho(r);
+        if (hd[q] >= 0 && rw[q].x == rC.x + wt[q]) acc += rec_rho(rw[q]);
+      if (hd[3] < -1) {  // arcs beyond the third, in arc order
+        for (int e = ~hd[3]; e < wt[3]; e++) {
+          const int2 hw = __ldcg(a.arc_hw + e);
+          const int4 r = rec[hw.x];
+          if (r.x == rC.x + hw.y) acc += rec_rho(r);
+        }
       }
       finish_vertex(a, rec, vC, (double)rC.y, acc);
     }
@@ -1354,13 +1354,11 @@ __device__ __forceinline__ void dep_cta_pipe_body(const DepArgs &a, int slot, in
     itC = itB;
     vC = vB;
     rC = rB;
-    gC = gB;
-#pragma unroll
-    for (int q = 0; q < 4; q++) hC[q] = hB[q];
+    aC0 = aB0;
+    aC1 = aB1;
     itB = itA;
     vB = vA;
     rB = rA;
-    gB = gA;
     itA = itN;
     vA = vN;
   }
@@ -1683,6 +1681,7 @@ static DepArgs dep_args(DeviceState *d, int buf, const int32_t *src, int32_t ns)
   DepArgs a{};
   a.arc_rng = d->arc_rng;
   a.arc_hw = d->arc_hw;
+  a.arc4 = d->arc4;
   a.arc_off = d->arc_off;
   a.arc_head = d->arc_head;
   a.arc_w = d->arc_w;
@@ -1968,6 +1967,36 @@ __global__ void k_max_i32(const int32_t *__restrict__ x, int64_t n, int32_t *out
 }
 
 // ------------------------------------------------------------------------------- upload
+// Per vertex its first four arcs in CSR order as (head, weight) pairs in two int4 (one 32-byte
+// sector: the dependency pass reads a vertex's arcs with one request instead of a range lookup and
+// four pair loads).  Missing arcs have head -1.  A vertex with more than four arcs keeps three in
+// place and puts (~e, end) in the fourth pair: its remaining arcs are arc_hw[e, end), e >= 3.
+static std::vector<int4> arc4_of(const std::vector<int32_t> &off, const std::vector<int32_t> &head,
+                                 const std::vector<int32_t> &w) {
+  const size_t n = off.empty() ? 0 : off.size() - 1;
+  std::vector<int4> out(2 * n);
+  for (size_t v = 0; v < n; v++) {
+    int32_t p[8];
+    for (int q = 0; q < 4; q++) {
+      p[2 * q] = -1;
+      p[2 * q + 1] = 0;
+    }
+    const int32_t b = off[v], e = off[v + 1];
+    const int inl = e - b > 4 ? 3 : e - b;
+    for (int q = 0; q < inl; q++) {
+      p[2 * q] = head[b + q];
+      p[2 * q + 1] = w[b + q];
+    }
+    if (e - b > 4) {
+      p[6] = ~(b + 3);
+      p[7] = e;
+    }
+    out[2 * v] = make_int4(p[0], p[1], p[2], p[3]);
+    out[2 * v + 1] = make_int4(p[4], p[5], p[6], p[7]);
+  }
+  return out;
+}
+
 static DeviceState *new_state(Handle &h, int device) {
   device_release(h);
   const Index &ix = h.host;
@@ -2000,6 +2029,8 @@ static DeviceState *new_state(Handle &h, int device) {
     for (size_t e = 0; e < hw.size(); e++) hw[e] = make_int2(ix.arc_head[e], ix.arc_w[e]);
     d->arc_rng = dupload(d, rng, st);
     d->arc_hw = dupload(d, hw, st);
+    const std::vector<int4> a4 = arc4_of(ix.arc_off, ix.arc_head, ix.arc_w);
+    d->arc4 = dupload(d, a4, st);
     CK(cudaStreamSynchronize(st));  // the staging vectors die here
   }
   d->vid_of = dupload(d, ix.vid_of, st);
@@ -2187,7 +2218,7 @@ void device_release(Handle &h) {
   if (!d) return;
   cudaSetDevice(d->device);
   cudaDeviceSynchronize();
-  void *ptrs[] = {d->depth, d->send, d->arc_off, d->arc_head, d->arc_w, d->arc_rng, d->arc_hw, d->vid_of, d->tid_of, d->lab_off, d->dis,
+  void *ptrs[] = {d->depth, d->send, d->arc_off, d->arc_head, d->arc_w, d->arc_rng, d->arc_hw, d->arc4, d->vid_of, d->tid_of, d->lab_off, d->dis,
                   d->dis_sh, d->anc, d->aend, d->ch, d->bc_tid, d->bc_vid, d->err, d->sources};
   for (void *p : ptrs)
     if (p) cudaFree(p);

@@ -33,6 +33,7 @@ struct DeviceState {
   int32_t n = 0, n_pad = 0, hmax_pad = 0;
   int32_t *depth = nullptr, *send = nullptr, *arc_off = nullptr, *arc_head = nullptr, *arc_w = nullptr;
   int2 *arc_rng = nullptr, *arc_hw = nullptr;
+  int4 *arc4 = nullptr;  // per vertex 2 x int4: (head, weight) of its first four arcs (see k_dependency_cta_pipe)
   int32_t *vid_of = nullptr, *tid_of = nullptr, *dis = nullptr, *anc = nullptr, *aend = nullptr;
   int32_t packed_bits = 0;  // > 0: the packed-key label scan applies
   int32_t *dis_sh = nullptr;  // dis << packed_bits (packed kernel only)
