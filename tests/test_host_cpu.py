@@ -133,8 +133,8 @@ def scan_rows(ex, sources_vid):
 
 @pytest.mark.parametrize("n_target,seed,sc", [(2000, 1, 0.0), (900, 5, 0.02), (300, 8, 0.05), (6000, 11, 0.05)])
 def test_mhl_index_rows_match_oracle(n_target, seed, sc):
-    """the last case has separators of more than 192 vertices, which the elimination merges into
-    their neighbours' lists in parallel"""
+    """separators of 32 or more vertices (all but the smallest cases) are merged into their
+    neighbours' lists in parallel"""
     n, u, v, w = grid_lines(n_target, seed=seed, shortcut_frac=sc)
     g = Q.Graph(nthreads=4)
     g.ReadLines(n, u, v, w)
@@ -186,6 +186,31 @@ def test_min_degree_order_is_permutation():
     g.ReadLines(n, u, v, w)
     o = g.min_degree_order()
     assert sorted(o.tolist()) == list(range(n))
+
+
+@pytest.mark.parametrize("n,seed,shortcuts", [(500, 2, 0.0), (700, 5, 0.05)])
+def test_min_degree_order_rule(n, seed, shortcuts):
+    """the elimination takes the vertex of least current degree (fill-in included), the smaller id
+    on ties -- restated here with neighbour sets and checked step by step (the library keeps the
+    remaining vertices in an indexed heap and merges large separators on several threads)"""
+    n, u, v, w = grid_lines(n, seed=seed, shortcut_frac=shortcuts)
+    g = Q.Graph()
+    g.ReadLines(n, u, v, w)
+    got = np.argsort(g.min_degree_order())  # elimination sequence
+    adj = [set() for _ in range(n)]
+    for a, b in zip(u, v):
+        if a != b:
+            adj[a - 1].add(b - 1)
+    alive = set(range(n))
+    for step in range(n):
+        x = min(alive, key=lambda y: (len(adj[y]), y))
+        assert got[step] == x, step
+        nb = adj[x]
+        for y in nb:
+            adj[y].discard(x)
+            adj[y] |= nb - {y}
+        alive.discard(x)
+        adj[x] = set()
 
 
 def test_scan_entries_matches_lca_depth_sum():
