@@ -109,6 +109,26 @@ def test_dependency_forms_agree(g2k, form):
     assert rel_err(bc, tc.bc(arcs, srcs)) <= BC_RTOL
 
 
+@pytest.mark.parametrize("form", [1, 2, 3, 4])
+def test_deep_dag_layer_counters_in_global_memory(form):
+    """a 2,500-vertex path: hop layers up to 2,499 exceed the shared-memory layer counters of the
+    CTA-per-source forms (2,046 layers for the pipelined one) and the warp forms' queues, so those
+    count layers in their per-slot global arrays.  One shortest path per pair, so
+    BC(v_i) = i * (n - 1 - i) exactly."""
+    n = 2500
+    nn, u, v, w = lines_of([(i, i + 1, 1 + i % 7) for i in range(n - 1)], n)
+    g = Q.Graph(device=0)
+    g.ReadLines(nn, u, v, w)
+    idx = g.build_index()
+    idx.set_tuning(dep_form=form)
+    try:
+        bc = idx.bc_all()
+    finally:
+        idx.set_tuning()
+    i = np.arange(n, dtype=np.float64)
+    assert np.allclose(bc, i * (n - 1 - i), rtol=1e-12, atol=0)
+
+
 def test_bc_repeatable_and_chunked(g2k):
     n, u, v, w, g, idx, tc, arcs = g2k
     a = idx.bc_all()
