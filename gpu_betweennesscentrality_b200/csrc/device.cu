@@ -2069,6 +2069,7 @@ static void finish_state(Handle &h, DeviceState *d) {
 }
 
 void device_upload(Handle &h, int device) {
+  NvtxRange nvtx("qbc.upload");
   if (!h.host.rows_on_host) {
     if (!h.dev) throw Error(QBC_EINVAL, "index rows exist only on a released device");
     device_download_rows(h);
@@ -2093,6 +2094,7 @@ void device_upload(Handle &h, int device) {
 }
 
 void device_build(Handle &h, int device, const Separators &seps) {
+  NvtxRange nvtx("qbc.build_device");
   Index &ix = h.host;
   try {
     DeviceState *d = new_state(h, device);
@@ -2267,6 +2269,7 @@ void check_err(DeviceState *d) {
 // Sorts nothing on the device: chunks take the source list in the given order; sources listed in
 // increasing tid order group nearby tree nodes into one CTA.
 void device_bc_sources(Handle &h, const int32_t *d_sources0, int32_t ns, double *d_bc_vid, void *stream) {
+  NvtxRange nvtx("qbc.bc_sources_device");
   DeviceState *d = need_dev(h);
   cudaStream_t user = stream ? (cudaStream_t)stream : d->s_label;
   CK(cudaEventRecord(d->ev_start, user));
@@ -2345,6 +2348,7 @@ static std::vector<int32_t> tid_sorted(const Index &ix, const int32_t *sources0,
 }
 
 void host_bc_sources(Handle &h, const int32_t *sources0, int32_t ns, double *bc_out) {
+  NvtxRange nvtx("qbc.bc_sources");
   DeviceState *d = need_dev(h);
   std::vector<int32_t> srt = tid_sorted(h.host, sources0, ns);
   int32_t *ds = stage_sources(d, srt.data(), ns, d->n);
@@ -2356,6 +2360,7 @@ void host_bc_sources(Handle &h, const int32_t *sources0, int32_t ns, double *bc_
 }
 
 void host_bc_plain(Handle &h, const int32_t *sources0, int32_t ns, double *bc_out) {
+  NvtxRange nvtx("qbc.bc_plain");
   DeviceState *d = need_dev(h);
   int32_t *ds = stage_sources(d, sources0, ns, d->n);
   cudaStream_t st = d->s_label;
@@ -2374,6 +2379,7 @@ void host_bc_plain(Handle &h, const int32_t *sources0, int32_t ns, double *bc_ou
 }
 
 void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, uint32_t *cnt, int32_t *hop) {
+  NvtxRange nvtx("qbc.rows");
   DeviceState *d = need_dev(h);
   cudaStream_t st = d->s_label;
   const int32_t n = d->n;

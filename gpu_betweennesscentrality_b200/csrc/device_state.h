@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <string>
 #include <utility>
@@ -12,6 +13,16 @@
 #include "device.h"
 
 namespace qbc {
+
+// NVTX range over a scope: the library's phases (index build, upload, sweeps, query batches, the
+// autotuner, served chunks) appear by name on Nsight timelines; with no tool attached a push/pop
+// is a check of one function pointer.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 #define CK(call)                                                                                    \
   do {                                                                                              \

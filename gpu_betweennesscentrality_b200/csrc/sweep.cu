@@ -205,6 +205,7 @@ static SweepPlan &plan_for(Handle &h, DeviceState *d, const int32_t *sources0, i
 }
 
 void host_bc_sweep(Handle &h, const int32_t *sources0, int32_t ns, double *bc_out) {
+  NvtxRange nvtx("qbc.bc_sweep");
   DeviceState *d = need_dev(h);
   SweepPlan &p = plan_for(h, d, sources0, ns);
   cudaStream_t st = d->s_label;
@@ -216,6 +217,7 @@ void host_bc_sweep(Handle &h, const int32_t *sources0, int32_t ns, double *bc_ou
 }
 
 void host_query_batch(Handle &h, const int32_t *points0, int64_t total, const int32_t *sources0, int32_t ns, double *out) {
+  NvtxRange nvtx("qbc.query_batch");
   DeviceState *d = need_dev(h);
   for (int64_t i = 0; i < total; i++)
     if (points0[i] < 0 || points0[i] >= h.host.n) throw Error(QBC_EINVAL, "query id " + std::to_string(points0[i]) + " out of range");
@@ -283,6 +285,7 @@ static bool label_fits(const Handle &h, const DeviceState *d, int32_t lanes, int
 }
 
 void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_source) {
+  NvtxRange nvtx("qbc.autotune");
   DeviceState *d = need_dev(h);
   std::vector<int32_t> tids = source_tids(h.host, sources0, ns);
   if (tids.empty()) throw Error(QBC_EINVAL, "empty tuning sample");
@@ -568,6 +571,7 @@ void Server::loop() {
         continue;
       }
       const int slot = (int)(k & 1);
+      NvtxRange nvtx("qbc.serve.chunk");  // one turn of the loop: enqueue a chunk, finish the previous one
       if (entries_dirty) {
         int64_t m = 0;
         for (Req *r : active)
