@@ -85,3 +85,76 @@ def test_missing_file_refused(tmp_path):
     with pytest.raises(Q.QbcError) as e:
         Q.Index.load(str(tmp_path / "none.qbcidx"), device=None)
     assert e.value.code == capi.QBC_EIO
+
+
+FNV_BASIS, FNV_PRIME, M64 = 1469598103934665603, 1099511628211, (1 << 64) - 1
+
+
+def _word_hash(body: bytes) -> int:
+    """restatement of the version-2 checksum: FNV-1a's xor-multiply on 64-bit little-endian words
+    in four interleaved lanes, the last block zero-padded, lanes and byte count folded"""
+    pad = body + b"\0" * (-len(body) % 32)
+    words = np.frombuffer(pad, dtype="<u8").tolist()
+    lanes = [FNV_BASIS ^ q for q in range(4)]
+    for i, w in enumerate(words):
+        q = i & 3
+        lanes[q] = ((lanes[q] ^ w) * FNV_PRIME) & M64
+    h = FNV_BASIS
+    for q in range(4):
+        h = ((h ^ lanes[q]) * FNV_PRIME) & M64
+    return ((h ^ len(body)) * FNV_PRIME) & M64
+
+
+def _byte_fnv(body: bytes) -> int:
+    h = FNV_BASIS
+    for c in body:
+        h = ((h ^ c) * FNV_PRIME) & M64
+    return h
+
+
+def _small_index():
+    n, u, v, w = grid_lines(300, seed=6)
+    g = Q.Graph()
+    g.ReadLines(n, u, v, w)
+    return g.build_index(upload=False)
+
+
+def test_checksum_is_the_word_lane_fnv(tmp_path):
+    idx = _small_index()
+    p = str(tmp_path / "s.qbcidx")
+    idx.save(p)
+    raw = open(p, "rb").read()
+    assert raw[:8] == b"QBCIDX02" and int.from_bytes(raw[8:12], "little") == 2
+    assert int.from_bytes(raw[-8:], "little") == _word_hash(raw[:-8])
+
+
+def test_version1_files_still_load(tmp_path):
+    """the first format (same layout, magic QBCIDX01, version 1, byte-wise FNV-1a) is read as is"""
+    idx = _small_index()
+    p = str(tmp_path / "s.qbcidx")
+    idx.save(p)
+    body = bytearray(open(p, "rb").read()[:-8])
+    body[0:8] = b"QBCIDX01"
+    body[8:12] = (1).to_bytes(4, "little")
+    v1 = str(tmp_path / "v1.qbcidx")
+    open(v1, "wb").write(bytes(body) + _byte_fnv(bytes(body)).to_bytes(8, "little"))
+    _same(idx, Q.Index.load(v1, device=None))
+    body[len(body) // 3] ^= 0x01
+    open(v1, "wb").write(bytes(body) + _byte_fnv(bytes(body[:len(body) // 3])).to_bytes(8, "little"))
+    with pytest.raises(Q.QbcError) as e:
+        Q.Index.load(v1, device=None)
+    assert e.value.code == capi.QBC_EIO
+
+
+@pytest.mark.parametrize("where", [9, 40, -9, -20, -40])
+def test_any_changed_byte_is_refused(tmp_path, where):
+    """header, first words, and bytes of the zero-padded last block"""
+    idx = _small_index()
+    p = str(tmp_path / "s.qbcidx")
+    idx.save(p)
+    raw = bytearray(open(p, "rb").read())
+    raw[where] ^= 0x10
+    open(p, "wb").write(bytes(raw))
+    with pytest.raises(Q.QbcError) as e:
+        Q.Index.load(p, device=None)
+    assert e.value.code == capi.QBC_EIO
