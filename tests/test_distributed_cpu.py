@@ -74,3 +74,40 @@ def test_shard_sources_partition():
     assert np.array_equal(np.concatenate(parts), order)
     with pytest.raises(ValueError):
         shard_sources(order, 2, 2)
+
+
+def _rank_leaves(rank, world, port, out_dir):
+    """rank 1 joins the group, then leaves without taking part in the reduction; rank 0's
+    all-reduce of its partial BC must end with an error within the group's timeout, not hang"""
+    import sys
+    import time
+
+    sys.path.insert(0, ROOT)
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from gpu_betweennesscentrality_b200.shard import all_reduce_bc
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=15))
+    if rank == 1:
+        os._exit(0)
+    t0 = time.time()
+    try:
+        all_reduce_bc(torch.ones(64, dtype=torch.float64))
+        outcome = "completed"
+    except Exception as e:  # the peer is gone: gloo reports a closed connection or a timeout
+        outcome = "error: " + type(e).__name__
+    with open(os.path.join(out_dir, "rank0.txt"), "w") as f:
+        f.write(f"{outcome}\n{time.time() - t0:.2f}\n")
+    os._exit(0)
+
+
+def test_a_rank_that_leaves_ends_the_reduction_with_an_error(tmp_path):
+    world = 2
+    mp.start_processes(_rank_leaves, args=(world, _free_port(), str(tmp_path)), nprocs=world, start_method="spawn")
+    outcome, seconds = open(tmp_path / "rank0.txt").read().split("\n")[:2]
+    assert outcome.startswith("error"), outcome
+    assert float(seconds) < 30.0
