@@ -423,8 +423,12 @@ def main():
                             "dependency_ms_per_step": stats["dep_ms"] / args.steps,
                             "compute_roof": {"unit": "label entries/clk/SM", "achieved": ent_per_clk,
                                              "peak": 25.6, "frac": ent_per_clk / 25.6,
-                                             "note": "inner loop bound: 5 shared-memory wavefronts per 128 "
-                                                     "lane-entries (source-row LDS.128 + broadcast target row)"},
+                                             "issue_peak": 128.0 / 3.5,
+                                             "note": "inner-loop model roofs: 5 shared-memory wavefronts per 128 "
+                                                     "lane-entries (source-row LDS.128 + broadcast target row) "
+                                                     "gives 25.6; 3.5 instructions per pair-entry at 128 lane-"
+                                                     "instructions/clk/SM gives issue_peak; kernels moving 40-60 % "
+                                                     "fewer wavefronts measured no faster, so issue and latency bind"},
                             "note": "algorithmic bytes = 12 B per label entry scanned + 12 B per target "
                                     "written; target rows are fetched once per 32-source group, so achieved "
                                     "exceeds HBM peak and DRAM traffic (profiles/) stays far below it"},
