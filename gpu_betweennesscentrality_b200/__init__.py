@@ -20,9 +20,10 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from .capi import (QBC_INDEX_H2H, QBC_INDEX_MHL, QbcError, check, f64p, i32, i32p, i64p, lib, ptr, u32p)
+from .capi import (QBC_INDEX_CSR, QBC_INDEX_H2H, QBC_INDEX_MHL, QbcError, check, f64p, i32, i32p, i64p, lib, ptr,
+                   u32p)
 
-__all__ = ["Graph", "Index", "QbcError", "QBC_INDEX_MHL", "QBC_INDEX_H2H", "read_order", "read_query"]
+__all__ = ["Graph", "Index", "QbcError", "QBC_INDEX_MHL", "QBC_INDEX_H2H", "QBC_INDEX_CSR", "read_order", "read_query"]
 
 
 class _GraphHandle:
@@ -151,12 +152,12 @@ class Index:
         return int(e.value)
 
     TUNING_KEYS = ("lanes_per_source", "label_threads", "split", "chunk", "dep_threads", "dep_form", "queue_depth",
-                   "label_warps", "label_tile", "label_passes")
+                   "label_warps", "label_tile", "label_passes", "sweep_delta", "sweep_threads")
 
     def set_tuning(self, lanes_per_source=0, label_threads=256, split=0, chunk=0, dep_threads=256, dep_form=0,
-                   queue_depth=0, label_warps=0, label_tile=0, label_passes=0):
+                   queue_depth=0, label_warps=0, label_tile=0, label_passes=0, sweep_delta=0, sweep_threads=0):
         p = i32([lanes_per_source, label_threads, split, chunk, dep_threads, dep_form, queue_depth, label_warps,
-                 label_tile, label_passes])
+                 label_tile, label_passes, sweep_delta, sweep_threads])
         check(lib().qbc_index_set_tuning(self.h, ptr(p, i32p), len(self.TUNING_KEYS)))
 
     def get_tuning(self):
@@ -284,7 +285,8 @@ class Graph:
 
     def build_index(self, kind=QBC_INDEX_MHL, node_order=None, upload: bool = True, on_device: bool = False) -> Index:
         """Builds the index on the host and uploads it to ``self.device`` unless ``upload`` is False;
-        with ``on_device`` the label rows are filled on ``self.device`` instead."""
+        with ``on_device`` the label rows are filled on ``self.device`` instead.  ``QBC_INDEX_CSR``
+        keeps no labels (rows come from shortest-path sweeps over the arc list on the device)."""
         if self._g is None:
             raise QbcError(1, "ReadGraph first")
         self.index = Index(self._g, kind, node_order, self.nthreads, self.device if (upload or on_device) else None,

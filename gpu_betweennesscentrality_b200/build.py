@@ -62,7 +62,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     nvcc, cxx = _nvcc(), _cxx()
     headers = [os.path.join(CSRC, h) for h in ("host.h", "device.h", "device_state.h")] + [os.path.join(INCLUDE, "qbc_b200.h")]
     objs = []
-    for src, kind in (("host.cpp", "cxx"), ("index_file.cpp", "cxx"), ("capi.cpp", "cxx"), ("device.cu", "cu"), ("sweep.cu", "cu")):
+    for src, kind in (("host.cpp", "cxx"), ("index_file.cpp", "cxx"), ("capi.cpp", "cxx"), ("device.cu", "cu"), ("sssp.cu", "cu"), ("sweep.cu", "cu")):
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         objs.append(o)

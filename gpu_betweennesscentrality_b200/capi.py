@@ -13,7 +13,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libqbc_b200.so")
 
 QBC_OK, QBC_EINVAL, QBC_EIO, QBC_EGRAPH, QBC_ECUDA, QBC_ENOMEM, QBC_EDEVICE, QBC_ETIMEOUT, QBC_EBUSY = range(9)
-QBC_INDEX_MHL, QBC_INDEX_H2H = 0, 1
+QBC_INDEX_MHL, QBC_INDEX_H2H, QBC_INDEX_CSR = 0, 1, 2
 STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "EIO", 3: "EGRAPH", 4: "ECUDA", 5: "ENOMEM", 6: "EDEVICE",
                 7: "ETIMEOUT", 8: "EBUSY"}
 

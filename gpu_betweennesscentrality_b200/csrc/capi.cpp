@@ -47,6 +47,8 @@ void need(bool ok, const char *what) {
   if (!ok) throw qbc::Error(QBC_EINVAL, what);
 }
 
+constexpr int32_t kTuningFields = 12;  // qbc_index_set_tuning's params layout
+
 void not_serving(const qbc_index *idx) {
   if (idx->h.server) throw qbc::Error(QBC_EBUSY, "the index is serving requests: close its server first");
 }
@@ -132,6 +134,8 @@ int qbc_index_build(const qbc_graph *g, int kind, const int32_t *node_order, int
       need(node_order != nullptr, "H2H index needs a node order");
       std::vector<int32_t> o(node_order, node_order + g->g.n);
       p->h.host = qbc::build_h2h(g->g, o, nthreads);
+    } else if (kind == QBC_INDEX_CSR) {
+      p->h.host = qbc::build_csr(g->g);
     } else {
       throw qbc::Error(QBC_EINVAL, "unknown index kind");
     }
@@ -142,9 +146,15 @@ int qbc_index_build(const qbc_graph *g, int kind, const int32_t *node_order, int
 int qbc_index_build_device(const qbc_graph *g, int kind, const int32_t *node_order, int device, qbc_index **out) {
   return guarded([&] {
     need(g && out, "null argument");
-    need(kind == QBC_INDEX_MHL || kind == QBC_INDEX_H2H, "unknown index kind");
-    need(kind == QBC_INDEX_MHL || node_order != nullptr, "H2H index needs a node order");
+    need(kind == QBC_INDEX_MHL || kind == QBC_INDEX_H2H || kind == QBC_INDEX_CSR, "unknown index kind");
+    need(kind != QBC_INDEX_H2H || node_order != nullptr, "H2H index needs a node order");
     auto p = std::make_unique<qbc_index>();
+    if (kind == QBC_INDEX_CSR) {  // no label rows to fill: the arc list goes to the device as it is
+      p->h.host = qbc::build_csr(g->g);
+      qbc::device_upload(p->h, device);
+      *out = p.release();
+      return;
+    }
     qbc::Separators seps;
     std::vector<int32_t> o;
     if (node_order) o.assign(node_order, node_order + g->g.n);
@@ -245,7 +255,7 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
     need(idx && (nparams == 0 || params), "null argument");
     qbc::Tuning &t = idx->h.tuning;
     not_serving(idx);
-    int32_t *f[] = {&t.lanes_per_source, &t.label_threads, &t.split, &t.chunk, &t.dep_threads, &t.dep_form, &t.queue_depth, &t.label_warps, &t.label_tile, &t.label_passes};
+    int32_t *f[] = {&t.lanes_per_source, &t.label_threads, &t.split, &t.chunk, &t.dep_threads, &t.dep_form, &t.queue_depth, &t.label_warps, &t.label_tile, &t.label_passes, &t.sweep_delta, &t.sweep_threads};
     if (nparams > 0) {
       int32_t k = params[0];
       need(k == 0 || k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32, "lanes per source must be 0 or a power of two <= 32");
@@ -258,7 +268,9 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
            "label warps must be 0, 8, 12 (two-target kernel), 16 or 20");
     if (nparams > 8) need(params[8] >= 0, "label tile must be >= 0");
     if (nparams > 9) need(params[9] >= 0 && params[9] <= 2, "label passes must be 0, 1 or 2");
-    for (int32_t i = 0; i < nparams && i < 10; i++) *f[i] = params[i];
+    if (nparams > 10) need(params[10] >= 0, "sweep bucket width must be >= 0");
+    if (nparams > 11) need(params[11] == 0 || params[11] == 256 || params[11] == 512, "sweep threads must be 0, 256 or 512");
+    for (int32_t i = 0; i < nparams && i < kTuningFields; i++) *f[i] = params[i];
     if (nparams > 3 && t.chunk != old_chunk && idx->h.dev) qbc::device_set_chunk(idx->h, t.chunk);
   });
 }
@@ -267,8 +279,8 @@ int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams)
   return guarded([&] {
     need(idx && (nparams == 0 || params), "null argument");
     const qbc::Tuning &t = idx->h.tuning;
-    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes};
-    for (int32_t i = 0; i < nparams && i < 10; i++) params[i] = f[i];
+    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes, t.sweep_delta, t.sweep_threads};
+    for (int32_t i = 0; i < nparams && i < kTuningFields; i++) params[i] = f[i];
   });
 }
 
@@ -356,8 +368,8 @@ int qbc_autotune(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *p
     qbc::autotune(idx->h, sources0, ns, &ms);
     if (ms_per_source) *ms_per_source = ms;
     const qbc::Tuning &t = idx->h.tuning;
-    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes};
-    for (int32_t i = 0; params && i < nparams && i < 10; i++) params[i] = f[i];
+    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes, t.sweep_delta, t.sweep_threads};
+    for (int32_t i = 0; params && i < nparams && i < kTuningFields; i++) params[i] = f[i];
   });
 }
 

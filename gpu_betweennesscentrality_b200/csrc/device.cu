@@ -40,21 +40,6 @@ constexpr int kLayerCap = 4094;  // shared-memory layer counters; deeper DAGs us
 constexpr int kHopBatch = 8;   // hop loads in flight per thread in the dependency pass's layer sort
 constexpr unsigned kFull = 0xffffffffu;
 
-// Per-source rows (dist/sigma pairs, hop layers) of a buffer with ns source slots are stored
-// chunk-blocked: entry (slot, t) lives at ((t / 8) * ns + slot) * 8 + t % 8, so the 8-target
-// chunk of the 32 consecutive slots a warp produces is one contiguous block.  With ns = 1 this is
-// the plain row layout.
-__host__ __device__ __forceinline__ size_t blk(int slot, int t, int ns) {
-  return ((size_t)(t >> 3) * (size_t)ns + (size_t)slot) * 8 + (size_t)(t & 7);
-}
-
-template <class T>
-struct RowView {
-  T *p;
-  int slot, ns;
-  __device__ __forceinline__ T &operator[](int t) const { return p[blk(slot, t, ns)]; }
-};
-
 // ------------------------------------------------------------------------------- K1 + K2
 struct LabelArgs {
   const int32_t *__restrict__ dis;
@@ -1635,6 +1620,18 @@ static bool use_packed(const Handle &h, const DeviceState *d, bool plain) {
 
 static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t *src, int32_t ns, bool plain,
                          cudaStream_t st) {
+  if (h.host.kind == IndexKind::CSR) {  // no labels: shortest-path sweeps give the rows
+    std::pair<cudaEvent_t, cudaEvent_t> ev{};
+    if (d->profiling) {
+      ev = take_events(d->ev_lab, d->ev_lab_used);
+      CK(cudaEventRecord(ev.first, st));
+    }
+    launch_sweep_rows(h, d, d->rec[buf], d->hop[buf], d->order[buf], d->lcnt[buf], src, ns, st);
+    if (d->profiling) CK(cudaEventRecord(ev.second, st));
+    d->label_launches++;
+    d->launches++;
+    return;
+  }
   const bool packed = use_packed(h, d, plain);
   LabelPlan p = packed ? LabelPlan{1, 32, d->hmax_pad, 512, 1, 0} : plan_label(h, d, ns, plain);
   LabelArgs a{};
@@ -2041,6 +2038,12 @@ static DeviceState *new_state(Handle &h, int device) {
   d->vid_of = dupload(d, ix.vid_of, st);
   d->tid_of = dupload(d, ix.tid_of, st);
   d->lab_off = dupload(d, ix.lab_off, st);
+  {
+    double wsum = 0.0;
+    for (int32_t x : ix.arc_w) wsum += x;
+    const double mean = ix.arc_w.empty() ? 1.0 : wsum / (double)ix.arc_w.size();
+    d->sweep_delta_auto = (int32_t)std::min(1.0 * (1 << 28), std::max(1.0, 2.0 * mean));
+  }
   return d;
 }
 
@@ -2052,7 +2055,7 @@ static void finish_state(Handle &h, DeviceState *d) {
     int B = 1;
     while ((1 << B) < ix.tree_height) B++;
     const uint64_t room = (uint64_t)1 << (32 - B);
-    d->packed_bits = (B <= 16 && 2ull * (uint64_t)std::max(ix.max_label, 0) + 2 < room) ? B : 0;
+    d->packed_bits = (ix.kind != IndexKind::CSR && B <= 16 && 2ull * (uint64_t)std::max(ix.max_label, 0) + 2 < room) ? B : 0;
   }
   if (d->packed_bits) {  // label distances pre-shifted by B for the packed kernel (one add per entry)
     const int64_t L = ix.lab_off[ix.n];
@@ -2261,6 +2264,7 @@ void check_err(DeviceState *d) {
     throw Error(QBC_EDEVICE, e == ERR_DISCONNECTED ? "device: SP-DAG wave pass did not reach every vertex"
                              : e == ERR_BAD_SOURCE ? "device: source id out of range"
                              : e == ERR_COPY_TIMEOUT ? "device: label-row copy wait ran out"
+                             : e == ERR_SWEEP_BOUND ? "device: shortest-path sweep ran past its pass bound"
                                                    : "device: kernel error word " + std::to_string(e));
   }
 }
@@ -2396,7 +2400,7 @@ void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, ui
       k_vid_to_tid<<<(c + 255) / 256, 256, 0, st>>>(ds + off, d->tid_of, d->src[0], c, n, d->err);
       CK(cudaGetLastError());
       launch_label(h, d, 0, d->src[0], c, false, st);
-      if (h.host.kind == IndexKind::H2H && (cnt || hop)) {
+      if (h.host.kind != IndexKind::MHL && (cnt || hop)) {
         // sigma and waves by the Kahn pass; BC accumulation goes to a scratch target
         CK(cudaMemsetAsync(d->bc_tid, 0, (size_t)n * 8, st));
         launch_dep(h, d, 0, d->src[0], c, st);
@@ -2481,24 +2485,28 @@ void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *s
   CK(cudaMemsetAsync(bc_tid, 0, (size_t)d->n * 8, st));
   k_static_set_source<<<1, 1, 0, st>>>(src, h.host.tid_of[source0]);
   CK(cudaGetLastError());
-  const LabelPlan p = plan_label(h, d, 1, true);
-  LabelArgs la{};
-  la.dis = d->dis;
-  la.ch = d->ch;
-  la.anc = d->anc;
-  la.lab_off = d->lab_off;
-  la.depth = d->depth;
-  la.send = d->send;
-  la.src = src;
-  la.ns = 1;
-  la.n = d->n;
-  la.n_pad = d->n_pad;
-  la.stride = p.S;
-  la.split = p.split;
-  la.out_rec = rec;
-  la.out_hop = hop;
-  if (h.host.kind == IndexKind::MHL) launch_label_c<true>(p, la, 1, st);
-  else launch_label_c<false>(p, la, 1, st);
+  if (h.host.kind == IndexKind::CSR) {  // label-free index: the shortest-path sweep gives the row
+    launch_sweep_rows(h, d, rec, hop, order, lcnt, src, 1, st);
+  } else {
+    const LabelPlan p = plan_label(h, d, 1, true);
+    LabelArgs la{};
+    la.dis = d->dis;
+    la.ch = d->ch;
+    la.anc = d->anc;
+    la.lab_off = d->lab_off;
+    la.depth = d->depth;
+    la.send = d->send;
+    la.src = src;
+    la.ns = 1;
+    la.n = d->n;
+    la.n_pad = d->n_pad;
+    la.stride = p.S;
+    la.split = p.split;
+    la.out_rec = rec;
+    la.out_hop = hop;
+    if (h.host.kind == IndexKind::MHL) launch_label_c<true>(p, la, 1, st);
+    else launch_label_c<false>(p, la, 1, st);
+  }
   DepArgs da{};
   da.arc_rng = d->arc_rng;
   da.arc_hw = d->arc_hw;

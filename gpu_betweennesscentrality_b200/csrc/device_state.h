@@ -32,7 +32,29 @@ struct NvtxRange {
                   std::string(#call) + ": " + cudaGetErrorString(e_));                              \
   } while (0)
 
-enum : int32_t { ERR_NONE = 0, ERR_HOP_CAP = 1, ERR_DISCONNECTED = 2, ERR_BAD_SOURCE = 3, ERR_COPY_TIMEOUT = 4 };
+enum : int32_t {
+  ERR_NONE = 0,
+  ERR_HOP_CAP = 1,
+  ERR_DISCONNECTED = 2,
+  ERR_BAD_SOURCE = 3,
+  ERR_COPY_TIMEOUT = 4,
+  ERR_SWEEP_BOUND = 5  // a shortest-path sweep ran past its pass bound
+};
+
+// Per-source rows (dist/sigma pairs, hop layers) of a buffer with ns source slots are stored
+// chunk-blocked: entry (slot, t) lives at ((t / 8) * ns + slot) * 8 + t % 8, so the 8-target
+// chunk of the 32 consecutive slots a warp produces is one contiguous block.  With ns = 1 this is
+// the plain row layout.
+__host__ __device__ __forceinline__ size_t blk(int slot, int t, int ns) {
+  return ((size_t)(t >> 3) * (size_t)ns + (size_t)slot) * 8 + (size_t)(t & 7);
+}
+
+template <class T>
+struct RowView {
+  T *p;
+  int slot, ns;
+  __device__ __forceinline__ T &operator[](int t) const { return p[blk(slot, t, ns)]; }
+};
 
 // ------------------------------------------------------------------------------- state
 struct SweepCache;  // captured sweep graphs (sweep.cu)
@@ -47,6 +69,7 @@ struct DeviceState {
   int4 *arc4 = nullptr;  // per vertex 2 x int4: (head, weight) of its first four arcs (see k_dependency_cta_pipe)
   int32_t *vid_of = nullptr, *tid_of = nullptr, *dis = nullptr, *anc = nullptr, *aend = nullptr;
   int32_t packed_bits = 0;  // > 0: the packed-key label scan applies
+  int32_t sweep_delta_auto = 1;  // CSR sweep's default bucket width (twice the mean arc weight)
   int32_t *dis_sh = nullptr;  // dis << packed_bits (packed kernel only)
   int64_t *lab_off = nullptr;
   int2 *ch = nullptr;
@@ -105,6 +128,11 @@ static T *dupload(DeviceState *d, const std::vector<T> &v, cudaStream_t s) {
 // scratch buffer `buf`: the label scan, then the dependency pass, which adds 0.5 * delta into
 // d->bc_tid (not cleared here).  Nothing in it synchronises, so it can be stream-captured.
 void launch_chunk(const Handle &h, DeviceState *d, const int32_t *d_src_tid, int32_t cnt, int buf, cudaStream_t st);
+// CSR index: rows (dist, sigma of the source) of ns sources by shortest-path sweeps into the given
+// scratch (rec/hop/order/lcnt laid out as a buffer of ns slots), one CTA per source (sssp.cu).
+void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop, int32_t *order, int32_t *lcnt,
+                       const int32_t *src, int32_t ns, cudaStream_t st);
+int32_t sweep_delta(const Handle &h, const DeviceState *d);
 // out_vid[vid_of[t]] (+)= in_tid[t] for all t
 void launch_tid_to_vid(DeviceState *d, const double *in_tid, double *out_vid, int accumulate, cudaStream_t st);
 // tids of cnt vids (sets ERR_BAD_SOURCE for ids out of range)

@@ -636,6 +636,51 @@ Index build_h2h(const Graph &g, const std::vector<int32_t> &node_order, int nthr
   return ix;
 }
 
+// Label-free index (IndexKind::CSR): the per-source rows come from shortest-path sweeps over the
+// arc list on the device, so the index is the arc list itself, kept in vertex-id order (tid = vid:
+// the file's own numbering, which for road graphs is usually spatially coherent, so a sweep's
+// frontier touches nearby rows).  No tree: depth 0, no parent, one-vertex "subtrees", no rows.
+// The graph must be connected (every BC path here assumes it, QBC.cu:525).
+Index build_csr(const Graph &g) {
+  const int32_t n = g.n;
+  if (n <= 0) throw Error(QBC_EGRAPH, "empty graph");
+  {
+    std::vector<int32_t> stack{0};
+    std::vector<char> seen((size_t)n, 0);
+    seen[0] = 1;
+    int32_t reached = 1;
+    while (!stack.empty()) {
+      const int32_t v = stack.back();
+      stack.pop_back();
+      for (int32_t e = g.off[v]; e < g.off[v + 1]; e++)
+        if (!seen[g.head[e]]) {
+          seen[g.head[e]] = 1;
+          reached++;
+          stack.push_back(g.head[e]);
+        }
+    }
+    if (reached != n)
+      throw Error(QBC_EGRAPH, "graph is not connected (" + std::to_string(n - reached) + " vertices unreachable from vertex 1)");
+  }
+  Index ix;
+  ix.kind = IndexKind::CSR;
+  ix.n = n;
+  ix.vid_of.resize((size_t)n);
+  ix.tid_of.resize((size_t)n);
+  ix.send.resize((size_t)n);
+  for (int32_t v = 0; v < n; v++) {
+    ix.vid_of[v] = ix.tid_of[v] = v;
+    ix.send[v] = v + 1;
+  }
+  ix.depth.assign((size_t)n, 0);
+  ix.parent.assign((size_t)n, -1);
+  ix.lab_off.assign((size_t)n + 1, 0);
+  ix.arc_off = g.off;
+  ix.arc_head = g.head;
+  ix.arc_w = g.w;
+  return ix;
+}
+
 std::vector<int32_t> min_degree_order(const Graph &g) {
   Elimination el = eliminate(g, nullptr);
   return el.rank;

@@ -32,7 +32,10 @@ Graph graph_read(const std::string &path);
 std::vector<int32_t> read_order(const std::string &path, int32_t n);
 std::vector<int32_t> read_query(const std::string &path, int32_t n);
 
-enum class IndexKind : int { MHL = 0, H2H = 1 };
+// MHL: TreeCount distance + count + hop labels; H2H: distance labels from an order file; CSR: no
+// labels (graphs whose tree decomposition is too wide), the per-source rows come from
+// shortest-path sweeps over the arc list.
+enum class IndexKind : int { MHL = 0, H2H = 1, CSR = 2 };
 
 // Tree-decomposition index in DFS-preorder numbering ("tid").  Row p holds one entry per
 // ancestor, root first, plus the node itself last (dis 0, cnt 1, hop 0); rows start on 4-entry
@@ -72,6 +75,8 @@ Index prepare_index(const Graph &g, IndexKind kind, const std::vector<int32_t> *
 Index build_mhl(const Graph &g, int nthreads);
 // H2H distance index from an order file (node_order[vid] = contraction rank).
 Index build_h2h(const Graph &g, const std::vector<int32_t> &node_order, int nthreads);
+// Label-free index: the arc list in vertex-id order (tid = vid), connectivity checked, no tree.
+Index build_csr(const Graph &g);
 // Min-degree contraction order (node_order[vid] = rank).
 std::vector<int32_t> min_degree_order(const Graph &g);
 

@@ -165,7 +165,9 @@ Index index_load(const std::string &path) {
   int64_t hdr2[2];
   f.get(hdr2, sizeof(hdr2));
   Index ix;
-  if (hdr[1] != (int32_t)IndexKind::MHL && hdr[1] != (int32_t)IndexKind::H2H) throw Error(QBC_EIO, path + ": bad index kind");
+  if (hdr[1] != (int32_t)IndexKind::MHL && hdr[1] != (int32_t)IndexKind::H2H && hdr[1] != (int32_t)IndexKind::CSR)
+    throw Error(QBC_EIO, path + ": bad index kind");
+  const bool csr = hdr[1] == (int32_t)IndexKind::CSR;  // arc list only: no tree, no rows
   ix.kind = (IndexKind)hdr[1];
   ix.n = hdr[2];
   const int32_t arcs = hdr[3];
@@ -174,7 +176,8 @@ Index index_load(const std::string &path) {
   ix.max_label = hdr[6];
   const int64_t L = hdr2[0];
   ix.depth_sum = hdr2[1];
-  if (ix.n <= 0 || arcs < 0 || L < 0 || ix.tree_height <= 0 || ix.tree_height > ix.n)
+  if (ix.n <= 0 || arcs < 0 || L < 0 ||
+      (csr ? (ix.tree_height != 0 || L != 0) : (ix.tree_height <= 0 || ix.tree_height > ix.n)))
     throw Error(QBC_EIO, path + ": corrupt index header");
   // the payload size the header implies must match the file before anything is allocated
   {
@@ -206,7 +209,12 @@ Index index_load(const std::string &path) {
   if (std::fread(&sum, 8, 1, f.f) != 1 || sum != want) throw Error(QBC_EIO, path + ": index file checksum mismatch");
   // structural checks the kernels rely on
   if (ix.lab_off[n] != L || ix.arc_off[n] != arcs) throw Error(QBC_EIO, path + ": inconsistent index arrays");
-  for (size_t t = 0; t < n; t++) {
+  for (size_t t = 0; t < n && csr; t++) {
+    if (ix.depth[t] != 0 || ix.parent[t] != -1 || ix.send[t] != (int32_t)t + 1 || ix.lab_off[t] != 0 ||
+        ix.vid_of[t] < 0 || ix.vid_of[t] >= ix.n || ix.tid_of[ix.vid_of[t]] != (int32_t)t || ix.arc_off[t] > ix.arc_off[t + 1])
+      throw Error(QBC_EIO, path + ": inconsistent index arrays");
+  }
+  for (size_t t = 0; t < n && !csr; t++) {
     if (ix.depth[t] < 1 || ix.depth[t] > ix.tree_height || ix.lab_off[t] % 4 != 0 ||
         ix.lab_off[t + 1] - ix.lab_off[t] < ix.depth[t] || ix.send[t] <= (int32_t)t || ix.send[t] > ix.n ||
         ix.vid_of[t] < 0 || ix.vid_of[t] >= ix.n || ix.tid_of[ix.vid_of[t]] != (int32_t)t ||

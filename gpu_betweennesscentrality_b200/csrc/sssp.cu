@@ -1,0 +1,245 @@
+// sssp.cu -- label-free per-source rows of libqbc_b200 (QBC_INDEX_CSR).
+//
+// The label kernels get a source's (distance, path count, max hop) row from ancestor labels of a
+// tree decomposition (MHLQBC.cu:334-412).  That index grows with the graph's tree width: on a road
+// grid with 2 % uniformly random long shortcuts the width jumps from 196 to 1,441 at 50k vertices
+// and the elimination (the reference's TreeDecomp::Reduce, TreeDecomp.cpp:54-208, as well as this
+// library's) does not finish at 200k.  For such graphs the rows come from a shortest-path sweep
+// over the arc list instead, one CTA per source:
+//
+//   k_sweep_dist   near-far bucketed shortest paths (distances only).  Vertices whose tentative
+//                  distance is below the current threshold T form the near list and are relaxed in
+//                  passes (Bellman-Ford inside the bucket) until no distance below T changes; a
+//                  relaxation that lands at or beyond T parks the vertex in the far list.  Then T
+//                  advances by the bucket width and the far list is split: entries now below T
+//                  become the next near list, entries settled earlier are dropped, the rest stay.
+//                  A vertex is relaxed again only when its distance dropped, and buckets keep the
+//                  long shortcuts (weights 500..5000 against ~100 on the grid) from flooding the
+//                  graph with distances that later get undercut.
+//
+// It writes the rows as records (dist, sigma = [t == s], 0, 0); the SP-DAG's counts and hop layers
+// then come from the device Kahn pass shared with the H2H index (k_kahn_dependency: sigma as 32-bit
+// wrapping sums over DAG predecessors, waves = the largest hop count over shortest paths, the
+// TreeCount count and my_cnt semantics), which also runs the dependency backprop.
+//
+// Scratch: the per-source buffers of the label path, used differently while the sweep runs:
+// tentative distances in the hop rows (4 B per vertex, 8 vertices per 32-byte sector: the hot
+// atomicMin target), stamps and the next near list in the layer-counter rows, the near list in the
+// level-queue rows, and the far list in the record rows (read as 32-int pages; the rows are only
+// written at the end).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <string>
+
+#include "device_state.h"
+
+namespace qbc {
+
+namespace {
+
+constexpr unsigned kSweepFull = 0xffffffffu;
+constexpr int kFarTile = 4;  // far-list entries per thread loaded before a compaction step writes
+
+struct SweepArgs {
+  const int4 *__restrict__ arc4;    // per vertex its first four arcs as (head, weight) pairs
+  const int2 *__restrict__ arc_hw;  // per arc (head, weight)
+  const int32_t *__restrict__ src;  // tids of this launch's sources, one per CTA
+  int32_t ns, n, n_pad;
+  int32_t delta;       // bucket width (distance units)
+  int32_t max_rounds;  // bound on passes and on far-list splits (error word beyond it)
+  int4 *rec;           // [ns][n_pad] output rows; the far list while sweeping
+  int32_t *dist;       // [ns][n_pad] tentative distances (the hop rows)
+  int32_t *order;      // [ns][n_pad] near list
+  int32_t *lcnt;       // [ns][2 (n_pad + 2)]: stamps, then the next near list
+  int32_t *err;
+};
+
+// far list i-th entry: the slot's record rows read as pages of 32 ints (8 records)
+struct FarList {
+  int4 *rec;
+  int slot, ns;
+  __device__ __forceinline__ int32_t &operator[](int i) const {
+    return reinterpret_cast<int32_t *>(rec + blk(slot, (i >> 5) << 3, ns))[i & 31];
+  }
+};
+
+// Shared state of one CTA's sweep.  stamp[u]: > 0 the pass whose next list holds u; < 0 the
+// (negated, minus one) split round whose far list holds u; 0 neither.
+struct SweepShared {
+  int near_len, next_len, far_len, min_kept;
+};
+
+__device__ __forceinline__ void relax(int u, int nd, const RowView<int32_t> &dist, int32_t *stamp, int T, int pass,
+                                      int far_tag, int32_t *next, const FarList &far, SweepShared &sh) {
+  if (nd >= dist[u]) return;  // a stale (larger) cached value only lets the atomic decide
+  const int old = atomicMin(&dist[u], nd);
+  if (nd >= old) return;
+  if (nd < T) {
+    if (atomicExch(stamp + u, pass) != pass) next[atomicAdd(&sh.next_len, 1)] = u;
+  } else if (atomicExch(stamp + u, far_tag) != far_tag) {
+    far[atomicAdd(&sh.far_len, 1)] = u;
+  }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_sweep_dist(SweepArgs a) {
+  __shared__ SweepShared sh;
+  const int slot = blockIdx.x;
+  if (slot >= a.ns) return;
+  const int s = a.src[slot];
+  const int tid = threadIdx.x;
+  const RowView<int32_t> dist{a.dist, slot, a.ns};
+  const RowView<int4> rec{a.rec, slot, a.ns};
+  int32_t *stamp = a.lcnt + (size_t)slot * 2 * (a.n_pad + 2);
+  int32_t *near = a.order + (size_t)slot * a.n_pad;
+  int32_t *next = stamp + (a.n_pad + 2);
+  const FarList far{a.rec, slot, a.ns};
+  for (int v = tid; v < a.n; v += THREADS) {
+    dist[v] = INT_MAX;
+    stamp[v] = 0;
+  }
+  if (tid == 0) {
+    sh.near_len = 1;
+    sh.next_len = 0;
+    sh.far_len = 0;
+    near[0] = s;
+  }
+  __syncthreads();
+  if (tid == 0) dist[s] = 0;
+  __syncthreads();
+  const int delta = a.delta;
+  int T = delta, pass = 0, round = 0;
+  bool bound_hit = false;
+  for (;;) {
+    // passes over the near list until no distance below T changes
+    for (;;) {
+      const int len = sh.near_len;
+      if (len == 0) break;
+      if (++pass > a.max_rounds) {
+        bound_hit = true;
+        break;
+      }
+      const int far_tag = -1 - round;
+      for (int i = tid; i < len; i += THREADS) {
+        const int v = near[i];
+        const int dv = dist[v];
+        const int4 p0 = __ldg(a.arc4 + 2 * v), p1 = __ldg(a.arc4 + 2 * v + 1);
+        if (p0.x >= 0) relax(p0.x, dv + p0.y, dist, stamp, T, pass, far_tag, next, far, sh);
+        if (p0.z >= 0) relax(p0.z, dv + p0.w, dist, stamp, T, pass, far_tag, next, far, sh);
+        if (p1.x >= 0) relax(p1.x, dv + p1.y, dist, stamp, T, pass, far_tag, next, far, sh);
+        if (p1.z >= 0) {
+          relax(p1.z, dv + p1.w, dist, stamp, T, pass, far_tag, next, far, sh);
+        } else if (p1.z < -1) {  // more than four arcs: the rest are arc_hw[~p1.z, p1.w)
+          for (int e = ~p1.z; e < p1.w; e++) {
+            const int2 hw = __ldg(a.arc_hw + e);
+            relax(hw.x, dv + hw.y, dist, stamp, T, pass, far_tag, next, far, sh);
+          }
+        }
+      }
+      __syncthreads();
+      if (tid == 0) {
+        sh.near_len = sh.next_len;
+        sh.next_len = 0;
+      }
+      int32_t *t = near;
+      near = next;
+      next = t;
+      __syncthreads();
+    }
+    if (bound_hit) break;
+    // split the far list at the next threshold; a split that moves nothing (an empty bucket)
+    // is repeated with the threshold just past the smallest distance left
+    int T_old = T;
+    T += delta;
+    bool moved = false;
+    while (!moved) {
+      const int flen = sh.far_len;
+      if (flen == 0 || ++round > a.max_rounds) break;
+      const int tag = -1 - round;
+      __syncthreads();  // every thread has read far_len
+      if (tid == 0) {
+        sh.far_len = 0;
+        sh.min_kept = INT_MAX;
+      }
+      __syncthreads();
+      for (int base = 0; base < flen; base += THREADS * kFarTile) {
+        int u[kFarTile], du[kFarTile];
+#pragma unroll
+        for (int q = 0; q < kFarTile; q++) {
+          const int i = base + q * THREADS + tid;
+          u[q] = i < flen ? far[i] : -1;
+        }
+#pragma unroll
+        for (int q = 0; q < kFarTile; q++) du[q] = u[q] >= 0 ? dist[u[q]] : 0;
+        __syncthreads();  // the tile is read before kept entries are written back in front of it
+        int mn = INT_MAX;
+#pragma unroll
+        for (int q = 0; q < kFarTile; q++) {
+          if (u[q] < 0 || du[q] < T_old) continue;  // settled in an earlier bucket: stale entry
+          if (du[q] < T) {
+            near[atomicAdd(&sh.near_len, 1)] = u[q];
+          } else {
+            far[atomicAdd(&sh.far_len, 1)] = u[q];
+            stamp[u[q]] = tag;
+            mn = min(mn, du[q]);
+          }
+        }
+        mn = __reduce_min_sync(kSweepFull, mn);
+        if ((tid & 31) == 0 && mn != INT_MAX) atomicMin(&sh.min_kept, mn);
+        __syncthreads();
+      }
+      moved = sh.near_len > 0;
+      if (!moved) {
+        T_old = T;
+        const int mk = sh.min_kept;
+        if (mk != INT_MAX) T = max(T + delta, (mk / delta + 1) * delta);
+      }
+    }
+    if (round > a.max_rounds) {
+      bound_hit = true;
+      break;
+    }
+    if (!moved) break;  // far list empty: every vertex is settled
+  }
+  if (bound_hit) {
+    if (tid == 0) atomicCAS(a.err, ERR_NONE, ERR_SWEEP_BOUND);
+    return;
+  }
+  // rows: (dist, sigma of the source) records for the Kahn pass; overwrites the far pages
+  for (int v = tid; v < a.n; v += THREADS) rec[v] = make_int4(dist[v], v == s ? 1 : 0, 0, 0);
+}
+
+}  // namespace
+
+// Bucket width: tuned, else twice the mean arc weight.  Capped so that thresholds stay far from
+// int32 overflow (distances are below 999,999,999, the graph reader's bound on total weight).
+int32_t sweep_delta(const Handle &h, const DeviceState *d) {
+  const int32_t w = h.tuning.sweep_delta > 0 ? h.tuning.sweep_delta : d->sweep_delta_auto;
+  return std::min<int32_t>(std::max<int32_t>(1, w), 1 << 28);
+}
+
+void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop, int32_t *order, int32_t *lcnt,
+                       const int32_t *src, int32_t ns, cudaStream_t st) {
+  SweepArgs a{};
+  a.arc4 = d->arc4;
+  a.arc_hw = d->arc_hw;
+  a.src = src;
+  a.ns = ns;
+  a.n = d->n;
+  a.n_pad = d->n_pad;
+  a.delta = sweep_delta(h, d);
+  // passes: at most one per vertex settled plus one per bucket; splits: one per bucket
+  a.max_rounds = 2 * d->n + 16;
+  a.rec = rec;
+  a.dist = hop;
+  a.order = order;
+  a.lcnt = lcnt;
+  a.err = d->err;
+  if (h.tuning.sweep_threads == 512) k_sweep_dist<512><<<ns, 512, 0, st>>>(a);
+  else k_sweep_dist<256><<<ns, 256, 0, st>>>(a);
+  CK(cudaGetLastError());
+}
+
+}  // namespace qbc

@@ -60,7 +60,7 @@ uint64_t fnv(uint64_t h, const void *p, size_t bytes) {
 
 uint64_t tuning_key(const Handle &h, const DeviceState *d) {
   const Tuning &t = h.tuning;
-  const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes, d->chunk};
+  const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes, t.sweep_delta, t.sweep_threads, d->chunk};
   return fnv(1469598103934665603ull, f, sizeof(f));
 }
 
@@ -327,6 +327,29 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
     };
     // 0. sources per scratch buffer (again at the end, after the kernels are chosen)
     chunk_trials();
+    if (h.host.kind == IndexKind::CSR) {
+      // label-free index: the sweep's bucket width (around twice the mean arc weight) and CTA
+      // size, then the Kahn/dependency pass's CTA size
+      const int32_t auto_delta = d->sweep_delta_auto;
+      for (int32_t mult : {1, 2, 4, 8, 16})
+        for (int32_t threads : {256, 512}) {
+          Tuning t = best;
+          t.sweep_delta = std::max(1, auto_delta * mult / 4);
+          t.sweep_threads = threads;
+          trial(t);
+        }
+      for (int32_t th : {128, 256}) {
+        Tuning t = best;
+        t.dep_threads = th;
+        trial(t);
+      }
+      chunk_trials();
+      h.tuning = best;
+      if (d->chunk != best.chunk) device_set_chunk(h, best.chunk);
+      *ms_per_source = best_t;
+      cudaFree(d_tids);
+      return;
+    }
     // 1. label kernel: the packed-key kernel with 8 or 16 warps (0 lanes) and, for tall trees, tile
     //    passes or a global-memory tail, or the general kernel
     //    with 32/K sources per CTA and 128 or 256 threads

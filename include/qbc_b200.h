@@ -35,7 +35,13 @@ enum {
 
 enum {
   QBC_INDEX_MHL = 0, /* TreeCount distance + count + hop labels (MHL-QBC, RQ) */
-  QBC_INDEX_H2H = 1  /* H2H distance labels from an order file (QBC) */
+  QBC_INDEX_H2H = 1, /* H2H distance labels from an order file (QBC) */
+  /* No labels: each source's (distance, count, hop) row comes from a shortest-path sweep over the
+   * arc list on the device (near-far buckets, then the SP-DAG counted in topological waves), the
+   * same rows the TreeCount scan gives (MHLQBC.cu:334-412 semantics).  For graphs whose tree
+   * decomposition is too wide for label rows, e.g. road grids with random long shortcuts, where
+   * the reference's own index build (TreeDecomp.cpp:54-208) does not finish. */
+  QBC_INDEX_CSR = 2
 };
 
 typedef struct qbc_graph qbc_graph; /* host arc list, Graph::ReadGraph rules */
@@ -68,7 +74,8 @@ int qbc_min_degree_order(const qbc_graph *g, int32_t *node_order);
 /* ---- index (replaces TreeDecomp Reduce/MakeTree/MakeIndex, src/TreeCount/TreeDecomp.cpp:54-511,
  * with moveCountIndexToDevice, MHLQBC.cu:6-128; and Graph::CHconsorderMT/makeTree/makeIndex,
  * src/buildIndex.cpp:4-310, with moveDisIndexToDevice, QBC.cu:11-127) -------------------------
- * kind QBC_INDEX_MHL ignores node_order; QBC_INDEX_H2H requires it.  nthreads <= 0: all cores. */
+ * kind QBC_INDEX_MHL ignores node_order; QBC_INDEX_H2H requires it; QBC_INDEX_CSR ignores it and
+ * keeps the arc list in vertex-id order (checked connected).  nthreads <= 0: all cores. */
 int qbc_index_build(const qbc_graph *g, int kind, const int32_t *node_order, int nthreads, qbc_index **out);
 /* copies the index to HBM of `device` (cudaSetDevice semantics, QBC.cu:601-602) */
 int qbc_index_upload(qbc_index *idx, int device);
@@ -113,7 +120,9 @@ int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int3
  * scan are read from global memory or taken in further passes, see [9]), [9]=label passes for
  * rows longer than the tile (0 = 1: one launch, entries beyond the tile read from global memory;
  * 2: one launch per tile of entries, the pairs' running minima kept in the output rows between
- * passes).  Refused with QBC_EBUSY while the index serves. */
+ * passes), [10]=distance bucket width of the CSR index's shortest-path sweep (0 = auto: twice the
+ * mean arc weight), [11]=threads per CTA of that sweep (256 or 512; 0 = 256).  Refused with
+ * QBC_EBUSY while the index serves. */
 int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams);
 int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams);
 
@@ -127,7 +136,8 @@ int qbc_index_stats(qbc_index *idx, double *out);
 /* Autotuner (no counterpart in the reference): times candidate tunings -- sources per CTA and
  * threads of the label kernel, target split, dependency form and level-queue depth, chunk size --
  * on a sweep over the listed sources, keeps the fastest on the index and returns it in params
- * (layout of qbc_index_set_tuning, up to 10) with its time per source in ms. */
+ * (layout of qbc_index_set_tuning, up to 12) with its time per source in ms.  On a CSR index
+ * it tunes the sweep's bucket width and threads, the dependency threads and the chunk size. */
 int qbc_autotune(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *params, int32_t nparams,
                  double *ms_per_source);
 

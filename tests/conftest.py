@@ -64,6 +64,11 @@ def graph_cache(tmp_path_factory):
 
 
 def rel_err(a, b):
+    """Largest relative difference |a - b| / |b|.  Entries of b near zero are measured against a
+    floor of 1e-12 * max|b| (a BC that is exactly 0 in b must be 0 in a up to that floor)."""
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
-    return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b)))) if a.size else 0.0
+    if not a.size:
+        return 0.0
+    floor = max(1e-12 * float(np.max(np.abs(b))), np.finfo(np.float64).tiny)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)))
