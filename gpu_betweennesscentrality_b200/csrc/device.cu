@@ -1626,7 +1626,7 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t
       ev = take_events(d->ev_lab, d->ev_lab_used);
       CK(cudaEventRecord(ev.first, st));
     }
-    launch_sweep_rows(h, d, d->rec[buf], d->hop[buf], d->order[buf], d->lcnt[buf], src, ns, st);
+    launch_sweep_rows(h, d, d->rec[buf], d->hop[buf], d->order[buf], d->lcnt[buf], d->maxhop[buf], src, ns, st);
     if (d->profiling) CK(cudaEventRecord(ev.second, st));
     d->label_launches++;
     d->launches++;
@@ -1705,7 +1705,9 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *
   // step; the pipelined warp form and the plain CTA form measured 153 and 151 ms, when this pass
   // took 146)
   const int form = h.tuning.dep_form == 0 ? 4 : h.tuning.dep_form;
-  const bool warp_form = h.host.kind == IndexKind::MHL && (form == 1 || form == 3) && !plain;
+  // MHL and CSR rows carry counts and hop layers; H2H rows are distances only (Kahn pass)
+  const bool counted = h.host.kind != IndexKind::H2H;
+  const bool warp_form = counted && (form == 1 || form == 3) && !plain;
   std::pair<cudaEvent_t, cudaEvent_t> ev{};
   if (d->profiling) {
     ev = take_events(d->ev_dp, d->ev_dp_used);
@@ -1722,9 +1724,9 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *
     if (form == 3)
       k_dependency_warp<true><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
     else k_dependency_warp<false><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
-  } else if (h.host.kind == IndexKind::MHL && form == 4 && !plain) {
+  } else if (counted && form == 4 && !plain) {
     k_dependency_cta_pipe<<<ns, threads, 0, st>>>(a, d->maxhop[buf]);
-  } else if (h.host.kind == IndexKind::MHL) {
+  } else if (counted) {
     k_dependency<<<ns, threads, 0, st>>>(a);
   } else {
     k_kahn_dependency<<<ns, threads, 0, st>>>(a);
@@ -2400,7 +2402,7 @@ void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, ui
       k_vid_to_tid<<<(c + 255) / 256, 256, 0, st>>>(ds + off, d->tid_of, d->src[0], c, n, d->err);
       CK(cudaGetLastError());
       launch_label(h, d, 0, d->src[0], c, false, st);
-      if (h.host.kind != IndexKind::MHL && (cnt || hop)) {
+      if (h.host.kind == IndexKind::H2H && (cnt || hop)) {
         // sigma and waves by the Kahn pass; BC accumulation goes to a scratch target
         CK(cudaMemsetAsync(d->bc_tid, 0, (size_t)n * 8, st));
         launch_dep(h, d, 0, d->src[0], c, st);
@@ -2486,7 +2488,7 @@ void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *s
   k_static_set_source<<<1, 1, 0, st>>>(src, h.host.tid_of[source0]);
   CK(cudaGetLastError());
   if (h.host.kind == IndexKind::CSR) {  // label-free index: the shortest-path sweep gives the row
-    launch_sweep_rows(h, d, rec, hop, order, lcnt, src, 1, st);
+    launch_sweep_rows(h, d, rec, hop, order, lcnt, nullptr, src, 1, st);
   } else {
     const LabelPlan p = plan_label(h, d, 1, true);
     LabelArgs la{};
@@ -2524,7 +2526,7 @@ void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *s
   da.bc = bc_tid;
   da.err = d->err;
   const int threads = std::max(64, std::min(256, (h.tuning.dep_threads / 32) * 32));
-  if (h.host.kind == IndexKind::MHL) k_dependency<<<1, threads, 0, st>>>(da);
+  if (h.host.kind != IndexKind::H2H) k_dependency<<<1, threads, 0, st>>>(da);  // rows carry counts and hops
   else k_kahn_dependency<<<1, threads, 0, st>>>(da);
   CK(cudaGetLastError());
   k_tid_to_vid_f64<<<(d->n + 255) / 256, 256, 0, st>>>(bc_tid, d->vid_of, d_bc_vid, d->n, 1);

@@ -128,10 +128,11 @@ static T *dupload(DeviceState *d, const std::vector<T> &v, cudaStream_t s) {
 // scratch buffer `buf`: the label scan, then the dependency pass, which adds 0.5 * delta into
 // d->bc_tid (not cleared here).  Nothing in it synchronises, so it can be stream-captured.
 void launch_chunk(const Handle &h, DeviceState *d, const int32_t *d_src_tid, int32_t cnt, int buf, cudaStream_t st);
-// CSR index: rows (dist, sigma of the source) of ns sources by shortest-path sweeps into the given
-// scratch (rec/hop/order/lcnt laid out as a buffer of ns slots), one CTA per source (sssp.cu).
+// CSR index: rows of ns sources by shortest-path sweeps into the given scratch (rec/hop/order/lcnt
+// laid out as a buffer of ns slots), one CTA per source (sssp.cu): records (dist, count, 0), hop
+// layers and, when maxhop is not null, the largest layer per source -- the label scan's outputs.
 void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop, int32_t *order, int32_t *lcnt,
-                       const int32_t *src, int32_t ns, cudaStream_t st);
+                       int32_t *maxhop, const int32_t *src, int32_t ns, cudaStream_t st);
 int32_t sweep_delta(const Handle &h, const DeviceState *d);
 // out_vid[vid_of[t]] (+)= in_tid[t] for all t
 void launch_tid_to_vid(DeviceState *d, const double *in_tid, double *out_vid, int accumulate, cudaStream_t st);

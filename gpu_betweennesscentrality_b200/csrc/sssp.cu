@@ -17,16 +17,19 @@
 //                  long shortcuts (weights 500..5000 against ~100 on the grid) from flooding the
 //                  graph with distances that later get undercut.
 //
-// It writes the rows as records (dist, sigma = [t == s], 0, 0); the SP-DAG's counts and hop layers
-// then come from the device Kahn pass shared with the H2H index (k_kahn_dependency: sigma as 32-bit
-// wrapping sums over DAG predecessors, waves = the largest hop count over shortest paths, the
-// TreeCount count and my_cnt semantics), which also runs the dependency backprop.
+//                  Then, in the same CTA, Kahn waves over the SP-DAG give each vertex's path count
+//                  (32-bit wrapping sum over its DAG predecessors) and hop layer (its wave: the
+//                  largest number of arcs on a shortest path) -- TreeCount's cnt and my_cnt.
+//
+// It writes the same outputs as the label scan -- records (dist, count, rho = 0), hop layers and
+// the largest layer per source -- so the dependency passes of the label path run unchanged.
 //
 // Scratch: the per-source buffers of the label path, used differently while the sweep runs:
 // tentative distances in the hop rows (4 B per vertex, 8 vertices per 32-byte sector: the hot
 // atomicMin target), stamps and the next near list in the layer-counter rows, the near list in the
 // level-queue rows, and the far list in the record rows (read as 32-int pages; the rows are only
-// written at the end).
+// written at the end).  The Kahn waves keep in-degrees and counts in the layer-counter rows and
+// their queue in the level-queue rows.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -53,6 +56,7 @@ struct SweepArgs {
   int32_t *dist;       // [ns][n_pad] tentative distances (the hop rows)
   int32_t *order;      // [ns][n_pad] near list
   int32_t *lcnt;       // [ns][2 (n_pad + 2)]: stamps, then the next near list
+  int32_t *maxhop;     // [ns] largest hop layer per source, or null
   int32_t *err;
 };
 
@@ -69,6 +73,7 @@ struct FarList {
 // (negated, minus one) split round whose far list holds u; 0 neither.
 struct SweepShared {
   int near_len, next_len, far_len, min_kept;
+  int tail;  // Kahn queue length
 };
 
 __device__ __forceinline__ void relax(int u, int nd, const RowView<int32_t> &dist, int32_t *stamp, int T, int pass,
@@ -207,8 +212,81 @@ __global__ void __launch_bounds__(THREADS) k_sweep_dist(SweepArgs a) {
     if (tid == 0) atomicCAS(a.err, ERR_NONE, ERR_SWEEP_BOUND);
     return;
   }
-  // rows: (dist, sigma of the source) records for the Kahn pass; overwrites the far pages
-  for (int v = tid; v < a.n; v += THREADS) rec[v] = make_int4(dist[v], v == s ? 1 : 0, 0, 0);
+  // ---- path counts and hop layers: Kahn waves over the SP-DAG (arcs t -> h with d[h] == d[t] + w).
+  // A vertex enters wave L once all its DAG predecessors are done, so L is the largest number of
+  // arcs on a shortest path (TreeCount's my_cnt) and its count, the 32-bit wrapping sum of its
+  // predecessors' counts, is complete (TreeCount's cnt).  All arrays are the compact 4-byte rows:
+  // in-degree, then the wave, in the stamp row; counts in the next-list row; the queue in the
+  // level-queue row.
+  int32_t *indeg = stamp;
+  int32_t *sig = stamp + (a.n_pad + 2);
+  int32_t *queue = a.order + (size_t)slot * a.n_pad;
+  for (int v = tid; v < a.n; v += THREADS) {
+    const int dv = dist[v];
+    const int4 p0 = __ldg(a.arc4 + 2 * v), p1 = __ldg(a.arc4 + 2 * v + 1);
+    int c = 0;
+    if (p0.x >= 0) c += dist[p0.x] + p0.y == dv;
+    if (p0.z >= 0) c += dist[p0.z] + p0.w == dv;
+    if (p1.x >= 0) c += dist[p1.x] + p1.y == dv;
+    if (p1.z >= 0) {
+      c += dist[p1.z] + p1.w == dv;
+    } else if (p1.z < -1) {
+      for (int e = ~p1.z; e < p1.w; e++) {
+        const int2 hw = __ldg(a.arc_hw + e);
+        c += dist[hw.x] + hw.y == dv;
+      }
+    }
+    indeg[v] = c;
+    sig[v] = v == s ? 1 : 0;
+  }
+  if (tid == 0) {
+    queue[0] = s;
+    sh.tail = 1;
+  }
+  __syncthreads();
+  int L = 0, b = 0, e = 1;
+  while (b < e) {
+    for (int i = b + tid; i < e; i += THREADS) {
+      const int v = queue[i];
+      const int dv = dist[v];
+      const int sv = sig[v];
+      indeg[v] = L;  // done: the slot now holds v's hop layer
+      auto push = [&](int h, int w) {
+        if (dist[h] != dv + w) return;
+        atomicAdd(sig + h, sv);                                              // 32-bit wrapping, as count_t
+        if (atomicSub(indeg + h, 1) == 1) queue[atomicAdd(&sh.tail, 1)] = h;  // its last predecessor
+      };
+      const int4 p0 = __ldg(a.arc4 + 2 * v), p1 = __ldg(a.arc4 + 2 * v + 1);
+      if (p0.x >= 0) push(p0.x, p0.y);
+      if (p0.z >= 0) push(p0.z, p0.w);
+      if (p1.x >= 0) push(p1.x, p1.y);
+      if (p1.z >= 0) {
+        push(p1.z, p1.w);
+      } else if (p1.z < -1) {
+        for (int q = ~p1.z; q < p1.w; q++) {
+          const int2 hw = __ldg(a.arc_hw + q);
+          push(hw.x, hw.y);
+        }
+      }
+    }
+    __syncthreads();
+    b = e;
+    e = sh.tail;
+    L++;
+    __syncthreads();  // every thread has read the tail before the next wave moves it
+  }
+  if (e != a.n) {  // a vertex the sweep did not reach (the index build rejects disconnected graphs)
+    if (tid == 0) atomicCAS(a.err, ERR_NONE, ERR_DISCONNECTED);
+    return;
+  }
+  if (tid == 0 && a.maxhop) a.maxhop[slot] = L - 1;  // waves 0 .. L-1 hold vertices
+  // rows: (dist, count, rho = 0) records and hop layers, as the label scan writes them; the far
+  // pages in the record rows and the distances in the hop rows are read before being overwritten
+  for (int v = tid; v < a.n; v += THREADS) {
+    const int dv = dist[v];
+    rec[v] = make_int4(dv, sig[v], 0, 0);
+    dist[v] = indeg[v];
+  }
 }
 
 }  // namespace
@@ -221,7 +299,7 @@ int32_t sweep_delta(const Handle &h, const DeviceState *d) {
 }
 
 void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop, int32_t *order, int32_t *lcnt,
-                       const int32_t *src, int32_t ns, cudaStream_t st) {
+                       int32_t *maxhop, const int32_t *src, int32_t ns, cudaStream_t st) {
   SweepArgs a{};
   a.arc4 = d->arc4;
   a.arc_hw = d->arc_hw;
@@ -236,6 +314,7 @@ void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop,
   a.dist = hop;
   a.order = order;
   a.lcnt = lcnt;
+  a.maxhop = maxhop;
   a.err = d->err;
   if (h.tuning.sweep_threads == 512) k_sweep_dist<512><<<ns, 512, 0, st>>>(a);
   else k_sweep_dist<256><<<ns, 256, 0, st>>>(a);

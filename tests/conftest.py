@@ -9,13 +9,22 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-# the reference's real road graph: read from the reference checkout when present, else from a
-# local, uncommitted copy under tests/golden/_data/
-LA_CANDIDATES = [os.path.join(GOLDEN, "_data", "LosAngeles.txt"), "/root/reference/data/roadData/LosAngeles.txt"]
-LA_ORDER_CANDIDATES = [os.path.join(GOLDEN, "_data", "LosAngelesOrder.txt"),
-                       "/root/reference/data/orderFile/LosAngelesOrder.txt"]
-LA_QUERY_CANDIDATES = [os.path.join(GOLDEN, "_data", "LosAngelesQuery.txt"),
-                       "/root/reference/data/queryBatch/LosAngeles.txt"]
+# the reference's real road graph: from the local, uncommitted copy under tests/golden/_data/ (the
+# oracle Makefile's `fixtures` target writes it from a reference checkout), else from the checkout
+# named by QBC_REFERENCE_DIR; the tests that need it skip when neither exists
+_REF_DIR = os.environ.get("QBC_REFERENCE_DIR", "")
+
+
+def _candidates(local, *rel):
+    c = [os.path.join(GOLDEN, "_data", local)]
+    if _REF_DIR:
+        c.append(os.path.join(_REF_DIR, *rel))
+    return c
+
+
+LA_CANDIDATES = _candidates("LosAngeles.txt", "data", "roadData", "LosAngeles.txt")
+LA_ORDER_CANDIDATES = _candidates("LosAngelesOrder.txt", "data", "orderFile", "LosAngelesOrder.txt")
+LA_QUERY_CANDIDATES = _candidates("LosAngelesQuery.txt", "data", "queryBatch", "LosAngeles.txt")
 
 
 def pytest_configure(config):
