@@ -5,31 +5,32 @@
 // grid with 2 % uniformly random long shortcuts the width jumps from 196 to 1,441 at 50k vertices
 // and the elimination (the reference's TreeDecomp::Reduce, TreeDecomp.cpp:54-208, as well as this
 // library's) does not finish at 200k.  For such graphs the rows come from a shortest-path sweep
-// over the arc list instead, one CTA per source:
+// over the arc list instead, one CTA per source (k_sweep_rows):
 //
-//   k_sweep_dist   near-far bucketed shortest paths (distances only).  Vertices whose tentative
-//                  distance is below the current threshold T form the near list and are relaxed in
-//                  passes (Bellman-Ford inside the bucket) until no distance below T changes; a
-//                  relaxation that lands at or beyond T parks the vertex in the far list.  Then T
-//                  advances by the bucket width and the far list is split: entries now below T
-//                  become the next near list, entries settled earlier are dropped, the rest stay.
-//                  A vertex is relaxed again only when its distance dropped, and buckets keep the
-//                  long shortcuts (weights 500..5000 against ~100 on the grid) from flooding the
-//                  graph with distances that later get undercut.
+//   distances  near-far buckets.  Vertices whose tentative distance is below the current threshold
+//              T form the near list and are relaxed in passes (Bellman-Ford inside the bucket)
+//              until no distance below T changes; a relaxation that lands at or beyond T parks the
+//              vertex in the far list.  Then T advances by the bucket width and the far list is
+//              split: entries now below T become the next near list, entries settled earlier are
+//              dropped, the rest stay.  A vertex is relaxed again only when its distance dropped,
+//              and the buckets keep the long shortcuts (weights 500..5000 against ~100 on the grid)
+//              from flooding the graph with distances that later get undercut.
+//   counts     Kahn waves over the SP-DAG (arcs t -> h with d[h] == d[t] + w): a vertex enters
+//              wave L once all its DAG predecessors are done, so L is the largest number of arcs
+//              on a shortest path (TreeCount's my_cnt) and its count, the 32-bit wrapping sum of
+//              its predecessors' counts, is complete (TreeCount's cnt).
 //
-//                  Then, in the same CTA, Kahn waves over the SP-DAG give each vertex's path count
-//                  (32-bit wrapping sum over its DAG predecessors) and hop layer (its wave: the
-//                  largest number of arcs on a shortest path) -- TreeCount's cnt and my_cnt.
+// It writes the same outputs as the label scan -- records (dist, count, .), hop layers and the
+// largest layer per source -- so the dependency passes of the label path run unchanged (they
+// write the records' last 8 bytes before reading them).
 //
-// It writes the same outputs as the label scan -- records (dist, count, rho = 0), hop layers and
-// the largest layer per source -- so the dependency passes of the label path run unchanged.
-//
-// Scratch: the per-source buffers of the label path, used differently while the sweep runs:
-// tentative distances in the hop rows (4 B per vertex, 8 vertices per 32-byte sector: the hot
-// atomicMin target), stamps and the next near list in the layer-counter rows, the near list in the
-// level-queue rows, and the far list in the record rows (read as 32-int pages; the rows are only
-// written at the end).  The Kahn waves keep in-degrees and counts in the layer-counter rows and
-// their queue in the level-queue rows.
+// Memory: the frontier phases visit vertices scattered over the graph (the shortcuts spread every
+// wave across it), so each visit costs DRAM sectors, not bytes.  A vertex's whole sweep state is
+// therefore its 16-byte record -- distance, list stamp (then count), in-degree -- and one sector
+// fetch serves a visit; measured at 1M vertices + 2 % shortcuts, separate 4-byte arrays for the
+// same fields cost 8-10 sectors per visit.  Lists use the per-source buffers of the label path:
+// near list and Kahn queue in the level-queue row, next near list and far list in the two halves
+// of the layer-counter row; hop layers go to the hop row as vertices leave their wave.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -52,67 +53,71 @@ struct SweepArgs {
   int32_t ns, n, n_pad;
   int32_t delta;       // bucket width (distance units)
   int32_t max_rounds;  // bound on passes and on far-list splits (error word beyond it)
-  int4 *rec;           // [ns][n_pad] output rows; the far list while sweeping
-  int32_t *dist;       // [ns][n_pad] tentative distances (the hop rows)
-  int32_t *order;      // [ns][n_pad] near list
-  int32_t *lcnt;       // [ns][2 (n_pad + 2)]: stamps, then the next near list
+  int4 *rec;           // [ns][n_pad] sweep state, then the output records
+  int32_t *hop;        // [ns][n_pad] hop layers out
+  int32_t *order;      // [ns][n_pad] near list, then the Kahn queue
+  int32_t *lcnt;       // [ns][2 (n_pad + 2)]: next near list, far list
   int32_t *maxhop;     // [ns] largest hop layer per source, or null
   int32_t *err;
 };
 
-// far list i-th entry: the slot's record rows read as pages of 32 ints (8 records)
-struct FarList {
-  int4 *rec;
-  int slot, ns;
-  __device__ __forceinline__ int32_t &operator[](int i) const {
-    return reinterpret_cast<int32_t *>(rec + blk(slot, (i >> 5) << 3, ns))[i & 31];
-  }
-};
-
-// Shared state of one CTA's sweep.  stamp[u]: > 0 the pass whose next list holds u; < 0 the
-// (negated, minus one) split round whose far list holds u; 0 neither.
+// Shared state of one CTA's sweep.  Record field y while sweeping: > 0 the pass whose next list
+// holds the vertex; < 0 the (negated, minus one) far-list split round whose far list holds it; 0
+// neither.
 struct SweepShared {
   int near_len, next_len, far_len, min_kept;
   int tail;  // Kahn queue length
 };
 
-__device__ __forceinline__ void relax(int u, int nd, const RowView<int32_t> &dist, int32_t *stamp, int T, int pass,
-                                      int far_tag, int32_t *next, const FarList &far, SweepShared &sh) {
-  if (nd >= dist[u]) return;  // a stale (larger) cached value only lets the atomic decide
-  const int old = atomicMin(&dist[u], nd);
+__device__ __forceinline__ void relax(const RowView<int4> &rec, int u, int nd, int T, int pass, int far_tag,
+                                      int32_t *next, int32_t *far, SweepShared &sh) {
+  int4 &r = rec[u];
+  if (nd >= r.x) return;  // a stale (larger) cached value only lets the atomic decide
+  const int old = atomicMin(&r.x, nd);
   if (nd >= old) return;
   if (nd < T) {
-    if (atomicExch(stamp + u, pass) != pass) next[atomicAdd(&sh.next_len, 1)] = u;
-  } else if (atomicExch(stamp + u, far_tag) != far_tag) {
+    if (atomicExch(&r.y, pass) != pass) next[atomicAdd(&sh.next_len, 1)] = u;
+  } else if (atomicExch(&r.y, far_tag) != far_tag) {
     far[atomicAdd(&sh.far_len, 1)] = u;
   }
 }
 
+// f(head, weight) for each arc of v in CSR order
+template <class F>
+__device__ __forceinline__ void for_arcs(const SweepArgs &a, int v, F &&f) {
+  const int4 p0 = __ldg(a.arc4 + 2 * v), p1 = __ldg(a.arc4 + 2 * v + 1);
+  if (p0.x >= 0) f(p0.x, p0.y);
+  if (p0.z >= 0) f(p0.z, p0.w);
+  if (p1.x >= 0) f(p1.x, p1.y);
+  if (p1.z >= 0) {
+    f(p1.z, p1.w);
+  } else if (p1.z < -1) {  // more than four arcs: the rest are arc_hw[~p1.z, p1.w)
+    for (int e = ~p1.z; e < p1.w; e++) {
+      const int2 hw = __ldg(a.arc_hw + e);
+      f(hw.x, hw.y);
+    }
+  }
+}
+
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) k_sweep_dist(SweepArgs a) {
+__global__ void __launch_bounds__(THREADS) k_sweep_rows(SweepArgs a) {
   __shared__ SweepShared sh;
   const int slot = blockIdx.x;
   if (slot >= a.ns) return;
   const int s = a.src[slot];
   const int tid = threadIdx.x;
-  const RowView<int32_t> dist{a.dist, slot, a.ns};
   const RowView<int4> rec{a.rec, slot, a.ns};
-  int32_t *stamp = a.lcnt + (size_t)slot * 2 * (a.n_pad + 2);
+  const RowView<int32_t> hop{a.hop, slot, a.ns};
   int32_t *near = a.order + (size_t)slot * a.n_pad;
-  int32_t *next = stamp + (a.n_pad + 2);
-  const FarList far{a.rec, slot, a.ns};
-  for (int v = tid; v < a.n; v += THREADS) {
-    dist[v] = INT_MAX;
-    stamp[v] = 0;
-  }
+  int32_t *next = a.lcnt + (size_t)slot * 2 * (a.n_pad + 2);
+  int32_t *far = next + (a.n_pad + 2);
+  for (int v = tid; v < a.n; v += THREADS) rec[v] = make_int4(v == s ? 0 : INT_MAX, 0, 0, 0);
   if (tid == 0) {
     sh.near_len = 1;
     sh.next_len = 0;
     sh.far_len = 0;
     near[0] = s;
   }
-  __syncthreads();
-  if (tid == 0) dist[s] = 0;
   __syncthreads();
   const int delta = a.delta;
   int T = delta, pass = 0, round = 0;
@@ -129,19 +134,8 @@ __global__ void __launch_bounds__(THREADS) k_sweep_dist(SweepArgs a) {
       const int far_tag = -1 - round;
       for (int i = tid; i < len; i += THREADS) {
         const int v = near[i];
-        const int dv = dist[v];
-        const int4 p0 = __ldg(a.arc4 + 2 * v), p1 = __ldg(a.arc4 + 2 * v + 1);
-        if (p0.x >= 0) relax(p0.x, dv + p0.y, dist, stamp, T, pass, far_tag, next, far, sh);
-        if (p0.z >= 0) relax(p0.z, dv + p0.w, dist, stamp, T, pass, far_tag, next, far, sh);
-        if (p1.x >= 0) relax(p1.x, dv + p1.y, dist, stamp, T, pass, far_tag, next, far, sh);
-        if (p1.z >= 0) {
-          relax(p1.z, dv + p1.w, dist, stamp, T, pass, far_tag, next, far, sh);
-        } else if (p1.z < -1) {  // more than four arcs: the rest are arc_hw[~p1.z, p1.w)
-          for (int e = ~p1.z; e < p1.w; e++) {
-            const int2 hw = __ldg(a.arc_hw + e);
-            relax(hw.x, dv + hw.y, dist, stamp, T, pass, far_tag, next, far, sh);
-          }
-        }
+        const int dv = rec[v].x;
+        for_arcs(a, v, [&](int u, int w) { relax(rec, u, dv + w, T, pass, far_tag, next, far, sh); });
       }
       __syncthreads();
       if (tid == 0) {
@@ -177,7 +171,7 @@ __global__ void __launch_bounds__(THREADS) k_sweep_dist(SweepArgs a) {
           u[q] = i < flen ? far[i] : -1;
         }
 #pragma unroll
-        for (int q = 0; q < kFarTile; q++) du[q] = u[q] >= 0 ? dist[u[q]] : 0;
+        for (int q = 0; q < kFarTile; q++) du[q] = u[q] >= 0 ? rec[u[q]].x : 0;
         __syncthreads();  // the tile is read before kept entries are written back in front of it
         int mn = INT_MAX;
 #pragma unroll
@@ -187,7 +181,7 @@ __global__ void __launch_bounds__(THREADS) k_sweep_dist(SweepArgs a) {
             near[atomicAdd(&sh.near_len, 1)] = u[q];
           } else {
             far[atomicAdd(&sh.far_len, 1)] = u[q];
-            stamp[u[q]] = tag;
+            rec[u[q]].y = tag;
             mn = min(mn, du[q]);
           }
         }
@@ -212,33 +206,15 @@ __global__ void __launch_bounds__(THREADS) k_sweep_dist(SweepArgs a) {
     if (tid == 0) atomicCAS(a.err, ERR_NONE, ERR_SWEEP_BOUND);
     return;
   }
-  // ---- path counts and hop layers: Kahn waves over the SP-DAG (arcs t -> h with d[h] == d[t] + w).
-  // A vertex enters wave L once all its DAG predecessors are done, so L is the largest number of
-  // arcs on a shortest path (TreeCount's my_cnt) and its count, the 32-bit wrapping sum of its
-  // predecessors' counts, is complete (TreeCount's cnt).  All arrays are the compact 4-byte rows:
-  // in-degree, then the wave, in the stamp row; counts in the next-list row; the queue in the
-  // level-queue row.
-  int32_t *indeg = stamp;
-  int32_t *sig = stamp + (a.n_pad + 2);
-  int32_t *queue = a.order + (size_t)slot * a.n_pad;
+  // ---- counts and hop layers: in-degrees over the DAG (vertex order: neighbours' records are
+  // mostly in the same or the next sectors), record (dist, count = [v == s], in-degree, 0)
   for (int v = tid; v < a.n; v += THREADS) {
-    const int dv = dist[v];
-    const int4 p0 = __ldg(a.arc4 + 2 * v), p1 = __ldg(a.arc4 + 2 * v + 1);
+    const int dv = rec[v].x;
     int c = 0;
-    if (p0.x >= 0) c += dist[p0.x] + p0.y == dv;
-    if (p0.z >= 0) c += dist[p0.z] + p0.w == dv;
-    if (p1.x >= 0) c += dist[p1.x] + p1.y == dv;
-    if (p1.z >= 0) {
-      c += dist[p1.z] + p1.w == dv;
-    } else if (p1.z < -1) {
-      for (int e = ~p1.z; e < p1.w; e++) {
-        const int2 hw = __ldg(a.arc_hw + e);
-        c += dist[hw.x] + hw.y == dv;
-      }
-    }
-    indeg[v] = c;
-    sig[v] = v == s ? 1 : 0;
+    for_arcs(a, v, [&](int h, int w) { c += rec[h].x + w == dv; });
+    rec[v] = make_int4(dv, v == s ? 1 : 0, c, 0);
   }
+  int32_t *queue = a.order + (size_t)slot * a.n_pad;
   if (tid == 0) {
     queue[0] = s;
     sh.tail = 1;
@@ -248,26 +224,14 @@ __global__ void __launch_bounds__(THREADS) k_sweep_dist(SweepArgs a) {
   while (b < e) {
     for (int i = b + tid; i < e; i += THREADS) {
       const int v = queue[i];
-      const int dv = dist[v];
-      const int sv = sig[v];
-      indeg[v] = L;  // done: the slot now holds v's hop layer
-      auto push = [&](int h, int w) {
-        if (dist[h] != dv + w) return;
-        atomicAdd(sig + h, sv);                                              // 32-bit wrapping, as count_t
-        if (atomicSub(indeg + h, 1) == 1) queue[atomicAdd(&sh.tail, 1)] = h;  // its last predecessor
-      };
-      const int4 p0 = __ldg(a.arc4 + 2 * v), p1 = __ldg(a.arc4 + 2 * v + 1);
-      if (p0.x >= 0) push(p0.x, p0.y);
-      if (p0.z >= 0) push(p0.z, p0.w);
-      if (p1.x >= 0) push(p1.x, p1.y);
-      if (p1.z >= 0) {
-        push(p1.z, p1.w);
-      } else if (p1.z < -1) {
-        for (int q = ~p1.z; q < p1.w; q++) {
-          const int2 hw = __ldg(a.arc_hw + q);
-          push(hw.x, hw.y);
-        }
-      }
+      const int4 r = rec[v];
+      hop[v] = L;
+      for_arcs(a, v, [&](int h, int w) {
+        int4 &rh = rec[h];
+        if (rh.x != r.x + w) return;
+        atomicAdd(&rh.y, r.y);                                            // 32-bit wrapping, as count_t
+        if (atomicSub(&rh.z, 1) == 1) queue[atomicAdd(&sh.tail, 1)] = h;  // its last predecessor
+      });
     }
     __syncthreads();
     b = e;
@@ -280,13 +244,6 @@ __global__ void __launch_bounds__(THREADS) k_sweep_dist(SweepArgs a) {
     return;
   }
   if (tid == 0 && a.maxhop) a.maxhop[slot] = L - 1;  // waves 0 .. L-1 hold vertices
-  // rows: (dist, count, rho = 0) records and hop layers, as the label scan writes them; the far
-  // pages in the record rows and the distances in the hop rows are read before being overwritten
-  for (int v = tid; v < a.n; v += THREADS) {
-    const int dv = dist[v];
-    rec[v] = make_int4(dv, sig[v], 0, 0);
-    dist[v] = indeg[v];
-  }
 }
 
 }  // namespace
@@ -311,13 +268,13 @@ void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop,
   // passes: at most one per vertex settled plus one per bucket; splits: one per bucket
   a.max_rounds = 2 * d->n + 16;
   a.rec = rec;
-  a.dist = hop;
+  a.hop = hop;
   a.order = order;
   a.lcnt = lcnt;
   a.maxhop = maxhop;
   a.err = d->err;
-  if (h.tuning.sweep_threads == 512) k_sweep_dist<512><<<ns, 512, 0, st>>>(a);
-  else k_sweep_dist<256><<<ns, 256, 0, st>>>(a);
+  if (h.tuning.sweep_threads == 256) k_sweep_rows<256><<<ns, 256, 0, st>>>(a);
+  else k_sweep_rows<512><<<ns, 512, 0, st>>>(a);
   CK(cudaGetLastError());
 }
 
