@@ -151,6 +151,13 @@ class Index:
         check(lib().qbc_index_scan_entries(self.h, ptr(s, i32p), int(s.shape[0]), C.byref(e)))
         return int(e.value)
 
+    def group_entries(self, sources: Sequence[int], group: int = 32) -> int:
+        """Label entries the batched scan copies from target rows for CTAs of ``group`` sources."""
+        s = i32(sources)
+        e = C.c_int64()
+        check(lib().qbc_index_group_entries(self.h, ptr(s, i32p), int(s.shape[0]), int(group), C.byref(e)))
+        return int(e.value)
+
     TUNING_KEYS = ("lanes_per_source", "label_threads", "split", "chunk", "dep_threads", "dep_form", "queue_depth",
                    "label_warps", "label_tile", "label_passes", "sweep_delta", "sweep_threads")
 

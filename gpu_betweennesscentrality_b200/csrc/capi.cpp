@@ -226,6 +226,15 @@ int qbc_index_scan_entries(const qbc_index *idx, const int32_t *sources0, int32_
   });
 }
 
+int qbc_index_group_entries(const qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t group, int64_t *entries) {
+  return guarded([&] {
+    need(idx && entries && (ns == 0 || sources0) && group > 0, "null argument or group < 1");
+    for (int32_t i = 0; i < ns; i++)
+      if (sources0[i] < 0 || sources0[i] >= idx->h.host.n) throw qbc::Error(QBC_EINVAL, "source id out of range");
+    *entries = qbc::group_entries(idx->h.host, sources0, ns, group);
+  });
+}
+
 void qbc_index_free(qbc_index *idx) { delete idx; }
 
 int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int32_t *send, int64_t *lab_off,

@@ -700,4 +700,25 @@ int64_t scan_entries(const Index &ix, const int32_t *sources0, int32_t ns) {
   return total;
 }
 
+// Label entries the packed-key scan copies from target rows: sources sorted by tid form CTAs of
+// `group` consecutive sources, and a CTA copies each target row t up to the deepest LCA depth of t
+// with any of its sources -- the depth of t's deepest ancestor-or-self that lies on some source's
+// root path (a preorder pass per group: parent before child).
+int64_t group_entries(const Index &ix, const int32_t *sources0, int32_t ns, int32_t group) {
+  std::vector<int32_t> tids((size_t)ns);
+  for (int32_t k = 0; k < ns; k++) tids[k] = ix.tid_of[sources0[k]];
+  std::sort(tids.begin(), tids.end());
+  std::vector<int32_t> mark((size_t)ix.n, -1), best((size_t)ix.n, 0);
+  int64_t total = 0;
+  for (int32_t g0 = 0; g0 < ns; g0 += group) {
+    for (int32_t k = g0; k < std::min(ns, g0 + group); k++)
+      for (int32_t a = tids[k]; a >= 0 && mark[a] != g0; a = ix.parent[a]) mark[a] = g0;
+    for (int32_t t = 0; t < ix.n; t++) {
+      best[t] = mark[t] == g0 ? ix.depth[t] : (ix.parent[t] >= 0 ? best[ix.parent[t]] : 0);
+      total += best[t];
+    }
+  }
+  return total;
+}
+
 }  // namespace qbc

@@ -82,6 +82,9 @@ std::vector<int32_t> min_degree_order(const Graph &g);
 
 // sum over targets of h(lca(s, t)) for each listed source (0-based vids)
 int64_t scan_entries(const Index &ix, const int32_t *sources0, int32_t ns);
+// label entries the packed-key scan copies from target rows for CTAs of `group` consecutive
+// sources (tid order): sum over groups and targets of the deepest LCA depth within the group
+int64_t group_entries(const Index &ix, const int32_t *sources0, int32_t ns, int32_t group);
 
 int hardware_threads(int requested);
 

@@ -99,6 +99,11 @@ int qbc_index_info(const qbc_index *idx, int64_t *info);
 /* Sum over the listed sources of the label entries the K2 scan reads (sum_t h(lca(s,t)));
  * the algorithmic-bytes figure of the roofline. */
 int qbc_index_scan_entries(const qbc_index *idx, const int32_t *sources0, int32_t ns, int64_t *entries);
+/* Label entries the batched label scan copies from target rows when the listed sources, sorted by
+ * tree position, form CTAs of `group` consecutive sources: each CTA copies target row t up to the
+ * deepest LCA depth of t with one of its sources.  Times 4 bytes, the DRAM-read model of that
+ * kernel's target rows (no counterpart in the reference, which reads labels per pair). */
+int qbc_index_group_entries(const qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t group, int64_t *entries);
 void qbc_index_free(qbc_index *idx);
 /* Copies the host index out (for inspection and tests).  Arrays sized by qbc_index_info:
  * vid_of/depth/send[n], lab_off[n+1], dis/anc[info[2]], ch[2*info[2]] (MHL only; may be NULL). */
