@@ -1626,7 +1626,10 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t
       ev = take_events(d->ev_lab, d->ev_lab_used);
       CK(cudaEventRecord(ev.first, st));
     }
-    launch_sweep_rows(h, d, d->rec[buf], d->hop[buf], d->order[buf], d->lcnt[buf], d->maxhop[buf], src, ns, st);
+    if (plain)  // one source over the whole GPU (the buffer's slot 0 has the plain row layout)
+      launch_sweep_rows_grid(h, d, d->rec[buf], d->hop[buf], d->order[buf], d->lcnt[buf], src, st);
+    else
+      launch_sweep_rows(h, d, d->rec[buf], d->hop[buf], d->order[buf], d->lcnt[buf], d->maxhop[buf], src, ns, st);
     if (d->profiling) CK(cudaEventRecord(ev.second, st));
     d->label_launches++;
     d->launches++;
@@ -2069,6 +2072,7 @@ static void finish_state(Handle &h, DeviceState *d) {
   d->bc_tid = dmalloc<double>(d, ix.n);
   d->bc_vid = dmalloc<double>(d, ix.n);
   d->err = dmalloc<int32_t>(d, 1);
+  d->grid_ctl = dmalloc<int32_t>(d, kGridCtlBytes / 4);
   CK(cudaMemsetAsync(d->err, 0, 4, st));
   CK(cudaStreamSynchronize(st));
 }
@@ -2231,7 +2235,7 @@ void device_release(Handle &h) {
   cudaSetDevice(d->device);
   cudaDeviceSynchronize();
   void *ptrs[] = {d->depth, d->send, d->arc_off, d->arc_head, d->arc_w, d->arc_rng, d->arc_hw, d->arc4, d->vid_of, d->tid_of, d->lab_off, d->dis,
-                  d->dis_sh, d->anc, d->aend, d->ch, d->bc_tid, d->bc_vid, d->err, d->sources};
+                  d->dis_sh, d->anc, d->aend, d->ch, d->bc_tid, d->bc_vid, d->err, d->grid_ctl, d->sources};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   free_scratch(d);
@@ -2449,7 +2453,8 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBy
 __global__ void k_static_set_source(int32_t *dst, int32_t tid) { *dst = tid; }
 
 // Address of g_static_scratch on `device`.  The symbol name is only a host-side stand-in, so
-// the device address is looked up once per device with that device current, and cached.
+// the device address is looked up once per device with that device current, and cached for the
+// life of the process (a cudaDeviceReset that recreates the device's context invalidates it).
 static unsigned char *static_scratch_on(int device) {
   static std::mutex mu;
   static std::vector<unsigned char *> cached;
@@ -2474,6 +2479,15 @@ void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *s
   if (source0 < 0 || source0 >= h.host.n) throw Error(QBC_EINVAL, "source id " + std::to_string(source0) + " out of range");
   if (!d_bc_vid) throw Error(QBC_EINVAL, "null BC output");
   DeviceState *d = need_dev(h);
+  if (h.host.kind != IndexKind::CSR) {
+    // the one-source label kernel keeps a source row and one row per warp in shared memory
+    // (44 B per tree level): taller trees need the batched path or a CSR index
+    const size_t budget = (size_t)std::max(48 * 1024, d->smem_optin) - 2048;
+    if ((size_t)44 * d->hmax_pad > budget)
+      throw Error(QBC_EINVAL, "tree height " + std::to_string(h.host.tree_height) + " exceeds the " +
+                                  std::to_string(budget / 44) + " levels the static-scratch entry point's label kernel holds in "
+                                  "shared memory; use qbc_bc_sources_device or a QBC_INDEX_CSR index");
+  }
   unsigned char *base = static_scratch_on(d->device);
   cudaStream_t st = stream ? (cudaStream_t)stream : d->s_label;
   int4 *rec = reinterpret_cast<int4 *>(base + kStaticRec);

@@ -86,6 +86,7 @@ struct DeviceState {
   int32_t *sources = nullptr;  // staging for host source lists
   int32_t sources_cap = 0;
   int32_t *err = nullptr;
+  int32_t *grid_ctl = nullptr;  // control block of the cooperative plain sweep (kGridCtlBytes)
   int64_t bytes = 0, scratch_bytes = 0;
   int smem_optin = 0;
   // optional per-launch timing of the two main kernels (events on their launching streams)
@@ -134,6 +135,11 @@ void launch_chunk(const Handle &h, DeviceState *d, const int32_t *d_src_tid, int
 void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop, int32_t *order, int32_t *lcnt,
                        int32_t *maxhop, const int32_t *src, int32_t ns, cudaStream_t st);
 int32_t sweep_delta(const Handle &h, const DeviceState *d);
+// CSR index, plain path: one source's rows (slot 0 of a one-slot buffer; no largest-layer output)
+// by a cooperative launch of the whole GPU
+constexpr size_t kGridCtlBytes = 256;
+void launch_sweep_rows_grid(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop, int32_t *order, int32_t *lcnt,
+                            const int32_t *src, cudaStream_t st);
 // out_vid[vid_of[t]] (+)= in_tid[t] for all t
 void launch_tid_to_vid(DeviceState *d, const double *in_tid, double *out_vid, int accumulate, cudaStream_t st);
 // tids of cnt vids (sets ERR_BAD_SOURCE for ids out of range)

@@ -246,6 +246,193 @@ __global__ void __launch_bounds__(THREADS) k_sweep_rows(SweepArgs a) {
   if (tid == 0 && a.maxhop) a.maxhop[slot] = L - 1;  // waves 0 .. L-1 hold vertices
 }
 
+// ------------------------------------------------------------------------------- plain path
+// One source swept by the whole GPU (the plain one-source-per-launch path): the same near-far
+// buckets and Kahn waves, every CTA of a cooperative launch working on one shared frontier.  The
+// lists' lengths live in a control block in global memory and the steps are separated by a grid
+// barrier.  Data written by other CTAs is read through L2 (__ldcg): their atomics do not update
+// this SM's L1.
+struct GridCtl {
+  unsigned arrive, gen;  // grid barrier: arrivals, generation
+  int abort;             // a barrier wait ran out: every CTA leaves at its next barrier
+  int near_len, next_len, far_len, keep_len, min_kept, tail;
+};
+
+constexpr long long kGridSpinLimit = 1ll << 24;  // ~2 s of 64-ns sleeps per barrier wait
+
+// Barrier over all CTAs of a cooperative launch with a bounded wait; false when the grid aborts.
+__device__ __forceinline__ bool grid_sync(GridCtl *c, unsigned &gen, int32_t *err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    if (atomicAdd(&c->arrive, 1u) == gridDim.x - 1) {
+      c->arrive = 0;
+      __threadfence();
+      atomicExch(&c->gen, gen + 1);
+    } else {
+      long long spins = 0;
+      while (*(volatile unsigned *)&c->gen == gen) {
+        if (*(volatile int *)&c->abort || ++spins > kGridSpinLimit) {
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+      if (!ok) {
+        atomicExch(&c->abort, 1);
+        atomicCAS(err, ERR_NONE, ERR_SWEEP_BOUND);
+      }
+    }
+    gen++;
+    __threadfence();
+    s_ok = ok && !*(volatile int *)&c->abort;
+  }
+  __syncthreads();
+  return s_ok;
+}
+
+__device__ __forceinline__ int ldcg(const int *p) { return __ldcg(p); }
+
+__device__ __forceinline__ void relax_grid(int4 *rec, int u, int nd, int T, int pass, int far_tag, int32_t *next,
+                                           int32_t *far, GridCtl *c) {
+  int *r = reinterpret_cast<int *>(rec + u);
+  if (nd >= ldcg(r)) return;
+  const int old = atomicMin(r, nd);
+  if (nd >= old) return;
+  if (nd < T) {
+    if (atomicExch(r + 1, pass) != pass) next[atomicAdd(&c->next_len, 1)] = u;
+  } else if (atomicExch(r + 1, far_tag) != far_tag) {
+    far[atomicAdd(&c->far_len, 1)] = u;
+  }
+}
+
+// rec/hop/order/lcnt: the single slot of a one-source buffer (plain rows); far lists ping-pong
+// between the second half of the layer-counter row and the hop row (written only by the waves)
+__global__ void __launch_bounds__(512) k_sweep_rows_grid(SweepArgs a, GridCtl *c) {
+  const int s = a.src[0];
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  int4 *rec = a.rec;
+  int32_t *near = a.order, *next = a.lcnt, *far = a.lcnt + (a.n_pad + 2), *far2 = a.hop;
+  unsigned gen = 0;
+  for (int v = gt; v < a.n; v += gs) __stcg(rec + v, make_int4(v == s ? 0 : INT_MAX, 0, 0, 0));
+  if (gt == 0) {
+    near[0] = s;
+    c->near_len = 1;
+  }
+  if (!grid_sync(c, gen, a.err)) return;
+  const int delta = a.delta;
+  int T = delta, pass = 0, round = 0;
+  for (;;) {
+    for (;;) {
+      const int len = ldcg(&c->near_len);
+      if (len == 0) break;
+      if (++pass > a.max_rounds) {
+        if (gt == 0) atomicCAS(a.err, ERR_NONE, ERR_SWEEP_BOUND);
+        return;  // uniform: every CTA read the same length and counts the same passes
+      }
+      const int far_tag = -1 - round;
+      for (int i = gt; i < len; i += gs) {
+        const int v = ldcg(near + i);
+        const int dv = ldcg(reinterpret_cast<const int *>(rec + v));
+        for_arcs(a, v, [&](int u, int w) { relax_grid(rec, u, dv + w, T, pass, far_tag, next, far, c); });
+      }
+      if (!grid_sync(c, gen, a.err)) return;
+      if (gt == 0) {
+        c->near_len = c->next_len;
+        c->next_len = 0;
+      }
+      int32_t *t = near;
+      near = next;
+      next = t;
+      if (!grid_sync(c, gen, a.err)) return;
+    }
+    int T_old = T;
+    T += delta;
+    bool moved = false;
+    while (!moved) {
+      const int flen = ldcg(&c->far_len);
+      if (flen == 0) break;
+      if (++round > a.max_rounds) {
+        if (gt == 0) atomicCAS(a.err, ERR_NONE, ERR_SWEEP_BOUND);
+        return;
+      }
+      const int tag = -1 - round;
+      if (gt == 0) {
+        c->keep_len = 0;
+        c->min_kept = INT_MAX;
+      }
+      if (!grid_sync(c, gen, a.err)) return;
+      for (int i = gt; i < flen + (gs - flen % gs) % gs; i += gs) {  // whole warps reach the reduction
+        int mn = INT_MAX;
+        if (i < flen) {
+          const int u = ldcg(far + i);
+          const int du = ldcg(reinterpret_cast<const int *>(rec + u));
+          if (du >= T_old) {
+            if (du < T) {
+              near[atomicAdd(&c->near_len, 1)] = u;
+            } else {
+              far2[atomicAdd(&c->keep_len, 1)] = u;
+              reinterpret_cast<int *>(rec + u)[1] = tag;
+              mn = du;
+            }
+          }
+        }
+        mn = __reduce_min_sync(kSweepFull, mn);
+        if ((threadIdx.x & 31) == 0 && mn != INT_MAX) atomicMin(&c->min_kept, mn);
+      }
+      if (!grid_sync(c, gen, a.err)) return;
+      if (gt == 0) c->far_len = c->keep_len;
+      int32_t *t = far;
+      far = far2;
+      far2 = t;
+      moved = ldcg(&c->near_len) > 0;
+      const int mk = ldcg(&c->min_kept);
+      if (!grid_sync(c, gen, a.err)) return;
+      if (!moved) {
+        T_old = T;
+        if (mk != INT_MAX) T = max(T + delta, (mk / delta + 1) * delta);
+      }
+    }
+    if (!moved) break;
+  }
+  // counts and hop layers (Kahn waves), as in k_sweep_rows
+  for (int v = gt; v < a.n; v += gs) {
+    const int dv = ldcg(reinterpret_cast<const int *>(rec + v));
+    int cnt = 0;
+    for_arcs(a, v, [&](int h, int w) { cnt += ldcg(reinterpret_cast<const int *>(rec + h)) + w == dv; });
+    __stcg(rec + v, make_int4(dv, v == s ? 1 : 0, cnt, 0));
+  }
+  int32_t *queue = a.order;
+  if (gt == 0) {
+    queue[0] = s;
+    c->tail = 1;
+  }
+  if (!grid_sync(c, gen, a.err)) return;
+  int L = 0, b = 0, e = 1;
+  while (b < e) {
+    for (int i = b + gt; i < e; i += gs) {
+      const int v = ldcg(queue + i);
+      const int dv = ldcg(reinterpret_cast<const int *>(rec + v));
+      const int sv = ldcg(reinterpret_cast<const int *>(rec + v) + 1);
+      a.hop[v] = L;
+      for_arcs(a, v, [&](int h, int w) {
+        int *rh = reinterpret_cast<int *>(rec + h);
+        if (ldcg(rh) != dv + w) return;
+        atomicAdd(rh + 1, sv);
+        if (atomicSub(rh + 2, 1) == 1) queue[atomicAdd(&c->tail, 1)] = h;
+      });
+    }
+    if (!grid_sync(c, gen, a.err)) return;
+    b = e;
+    e = ldcg(&c->tail);
+    L++;
+    if (!grid_sync(c, gen, a.err)) return;
+  }
+  if (e != a.n && gt == 0) atomicCAS(a.err, ERR_NONE, ERR_DISCONNECTED);
+}
+
 }  // namespace
 
 // Bucket width: tuned, else twice the mean arc weight.  Capped so that thresholds stay far from
@@ -276,6 +463,35 @@ void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop,
   if (h.tuning.sweep_threads == 256) k_sweep_rows<256><<<ns, 256, 0, st>>>(a);
   else k_sweep_rows<512><<<ns, 512, 0, st>>>(a);
   CK(cudaGetLastError());
+}
+
+void launch_sweep_rows_grid(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop, int32_t *order, int32_t *lcnt,
+                            const int32_t *src, cudaStream_t st) {
+  static_assert(sizeof(GridCtl) <= kGridCtlBytes, "grid control block");
+  SweepArgs a{};
+  a.arc4 = d->arc4;
+  a.arc_hw = d->arc_hw;
+  a.src = src;
+  a.ns = 1;
+  a.n = d->n;
+  a.n_pad = d->n_pad;
+  a.delta = sweep_delta(h, d);
+  a.max_rounds = 2 * d->n + 16;
+  a.rec = rec;
+  a.hop = hop;
+  a.order = order;
+  a.lcnt = lcnt;
+  a.maxhop = nullptr;
+  a.err = d->err;
+  // every CTA of the grid resident at once (the barrier waits on all of them)
+  int per_sm = 0, sms = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_rows_grid, 512, 0));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device));
+  if (per_sm < 1) throw Error(QBC_EDEVICE, "plain sweep kernel does not fit an SM");
+  GridCtl *c = reinterpret_cast<GridCtl *>(d->grid_ctl);
+  CK(cudaMemsetAsync(c, 0, sizeof(GridCtl), st));
+  void *args[] = {&a, &c};
+  CK(cudaLaunchCooperativeKernel((const void *)k_sweep_rows_grid, dim3((unsigned)(per_sm * sms)), dim3(512), args, 0, st));
 }
 
 }  // namespace qbc

@@ -167,12 +167,17 @@ int qbc_bc_sources_device(qbc_index *idx, const int32_t *d_sources0, int32_t ns,
  * cudaMalloc/cudaFree (they synchronise the device and have unbounded latency).  The per-source
  * scratch lives in a static device array built into the library (about 5 MiB, held by every GPU
  * that loads the library until the process exits), so graphs are limited to
- * QBC_STATIC_MAX_VERTICES vertices (larger ones return QBC_EINVAL).  The index must already be
- * uploaded.  Adds 0.5*delta_s(v) into d_bc (device pointer, n doubles, 0-based vid order) on
- * `stream` (NULL: the index's stream); the caller synchronises.  The first call on a device looks
- * up the array's device address with that device current; make that first call before any stream
- * capture.  All calls share the one array, which keeps the previous call's contents: calls that
- * overlap on the GPU (other streams, other host threads) race, so issue them in one stream. */
+ * QBC_STATIC_MAX_VERTICES vertices (larger ones return QBC_EINVAL).  On a label index the
+ * one-source label kernel also holds 44 bytes per tree level in shared memory, so trees taller
+ * than about 5,100 levels (long paths, thin strips) return QBC_EINVAL too; a QBC_INDEX_CSR index
+ * has no such limit.  The index must already be uploaded.  Adds 0.5*delta_s(v) into d_bc (device
+ * pointer, n doubles, 0-based vid order) on `stream` (NULL: the index's stream); the caller
+ * synchronises.  A device-side error of the call (a sweep that hit its bound) is recorded in the
+ * index's error word and returned by the index's next synchronous call.  The first call on a
+ * device looks up the array's device address with that device current and caches it for the
+ * process; make that first call before any stream capture, and not across a cudaDeviceReset.
+ * All calls share the one array, which keeps the previous call's contents: calls that overlap
+ * on the GPU (other streams, other host threads) race, so issue them in one stream. */
 #define QBC_STATIC_MAX_VERTICES 131072
 int qbc_bc_source_static(qbc_index *idx, int32_t source0, double *d_bc, void *stream);
 

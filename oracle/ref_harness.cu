@@ -4,8 +4,8 @@
 // -Dmain=ref_main and links it with this harness into oracle/_ref/ref_{mhlqbc,qbc,rq}.  The
 // reference CLIs print BC with %.2f (MHLQBC.cu:570, QBC.cu:617) or %.8f (RQ.cu:583); this
 // harness calls the same Graph methods and writes %.17g instead, plus wall times of the
-// CPU index build alone and of the whole driver call (index build + GPU), so that the GPU
-// share can be read as the difference.
+// CPU index build alone and of the whole driver call (index build + GPU); the *_timed builds also
+// report the reference kernels' own time (kernel_ms, CUDA events around each launch).
 //
 //   ref_mhlqbc <graph> <out>            Graph::brandesBCIndexGPU_5   (MHLQBC.cu:495)
 //   ref_qbc    <graph> <order> <out>    Graph::brandesBCIndexGPU_5   (QBC.cu:419)
@@ -14,6 +14,42 @@
 
 #include <chrono>
 #include <cstdio>
+#include <utility>
+#include <vector>
+
+#if defined(REF_KERNEL_TIMING)
+// Kernel time of the reference's own launches.  This harness is linked with the shared CUDA
+// runtime, so the reference's <<<>>> launches (compiled unmodified in its .o) bind to this
+// definition of cudaLaunchKernel, which brackets each launch with CUDA events on its stream and
+// forwards to the runtime's own function.
+#include <dlfcn.h>
+static std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_launch_events;
+extern "C" cudaError_t cudaLaunchKernel(const void *func, dim3 grid, dim3 block, void **args, size_t shmem,
+                                        cudaStream_t stream) {
+  using Fn = cudaError_t (*)(const void *, dim3, dim3, void **, size_t, cudaStream_t);
+  static Fn real = reinterpret_cast<Fn>(dlsym(RTLD_NEXT, "cudaLaunchKernel"));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, stream);
+  const cudaError_t e = real(func, grid, block, args, shmem, stream);
+  cudaEventRecord(b, stream);
+  g_launch_events.push_back({a, b});
+  return e;
+}
+static double kernel_ms() {
+  cudaDeviceSynchronize();
+  double ms = 0.0;
+  for (auto &p : g_launch_events) {
+    float x = 0.f;
+    cudaEventElapsedTime(&x, p.first, p.second);
+    ms += x;
+  }
+  return ms;
+}
+#else
+static double kernel_ms() { return -1.0; }
+#endif
 
 extern string roadDataPath;
 #if defined(REF_QBC)
@@ -89,7 +125,7 @@ int main(int argc, char **argv) {
 #endif
   fclose(f);
   cudaError_t err = cudaGetLastError();
-  printf("{\"n\": %d, \"arcs\": %d, \"index_s\": %.6f, \"total_s\": %.6f, \"cuda\": \"%s\"}\n", g.nodenum,
-         g.edgenum, t_idx, t1 - t0, cudaGetErrorString(err));
+  printf("{\"n\": %d, \"arcs\": %d, \"index_s\": %.6f, \"total_s\": %.6f, \"kernel_ms\": %.3f, \"cuda\": \"%s\"}\n",
+         g.nodenum, g.edgenum, t_idx, t1 - t0, kernel_ms(), cudaGetErrorString(err));
   return err == cudaSuccess ? 0 : 1;
 }

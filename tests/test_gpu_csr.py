@@ -111,6 +111,19 @@ def test_plain_path_equals_batched(g2k):
     assert rel_err(ref, arcs.bc(srcs)) <= BC_RTOL
 
 
+@pytest.mark.parametrize("delta", [0, 1, 1 << 20])
+def test_plain_whole_gpu_sweep_matches_batched_shortcut_graph(delta):
+    """the plain path sweeps one source with every CTA of a cooperative launch: same BC as the
+    one-CTA-per-source batched sweep and the oracle, for label-setting, default and single-bucket
+    widths"""
+    n, u, v, w = grid_lines(5000, seed=9, shortcut_frac=0.05)
+    idx = _csr(n, u, v, w, sweep_delta=delta)
+    srcs = np.array([0, 17, 2500, n - 1], np.int32)
+    ref = O.Arcs(n, u, v, w).bc(srcs)
+    assert rel_err(idx.bc_plain(srcs), ref) <= BC_RTOL
+    assert rel_err(idx.bc_sources(srcs), ref) <= BC_RTOL
+
+
 def test_query_batch_and_served_requests(g2k):
     n, u, v, w, idx, tc, arcs = g2k
     full = arcs.bc()

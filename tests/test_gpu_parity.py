@@ -176,6 +176,31 @@ def test_rq_2k(g2k):
         assert rel_err(o_, idx.bc_query(s_)) <= BC_RTOL
 
 
+def test_rq_follows_half_delta_where_the_pair_product_wraps():
+    """RQ of a query set is BC restricted to it (1/2 sum_s delta_s); on the 24 x 24 unit grid the
+    reference's int32 pair product (RQ.cu:456) wraps and its RQ departs from that value, which this
+    library keeps (label and label-free indexes)"""
+    n, u, v, w = unit_grid_lines()
+    q = np.array([0, 11, 24 * 11 + 11, 24 * 12 + 12, 300, n - 1], np.int32)
+    half_delta = O.Arcs(n, u, v, w).bc()[q]
+    g = _graph(n, u, v, w)
+    assert rel_err(g.build_index().bc_query(q), half_delta) <= BC_RTOL
+    assert rel_err(g.build_index(Q.QBC_INDEX_CSR).bc_query(q), half_delta) <= BC_RTOL
+
+
+def test_full_bc_50k_matches_reference_gpu_golden():
+    """all-source BC of the benchmark's 50k grid against the reference's own GPU driver
+    (MHLQBC.cu:495-537, run unmodified on a B200 by tests/golden/make_golden.py --g50k)"""
+    p = os.path.join(GOLDEN, "ref_g50k_mhl.npz")
+    if not os.path.exists(p):
+        pytest.skip("50k reference golden not generated")
+    ref = np.load(p)["bc"]
+    n, u, v, w = grid_lines(50000, seed=1)
+    g = _graph(n, u, v, w)
+    assert rel_err(g.build_index(on_device=True).bc_all(), ref) <= BC_RTOL
+    assert rel_err(g.build_index(Q.QBC_INDEX_CSR).bc_all(), ref) <= BC_RTOL
+
+
 @pytest.mark.parametrize("name", sorted(KNOWN))
 def test_known_graphs(name):
     n, edges, expect = KNOWN[name]

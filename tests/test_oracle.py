@@ -157,3 +157,25 @@ def test_oracle_matches_reference_gpu_la(la_path):
     n, u, v, w = synth.read_graph_lines(la_path)
     assert ref.shape[0] == n
     assert rel_err(O.Arcs(n, u, v, w).bc(), ref) <= BC_RTOL
+
+
+def test_rq_pair_product_wraps_where_half_delta_does_not():
+    """The reference's RQ pair kernel multiplies the two path counts as int32, (int)(sigma_vs *
+    sigma_vt) (RQ.cu:456), which wraps once the product passes 2^31; BC restricted to the query set
+    (1/2 sum_s delta_s(v), MHLQBC.cu's quantity, with the same 32-bit counts) has no such product.
+    Where counts stay small (the 2k grid) the two agree to 1e-9; on the 24 x 24 unit grid (counts up
+    to C(46,23)) the pair formula departs from it.  This library's RQ follows 1/2 sum delta."""
+    from util import unit_grid_lines
+
+    n, u, v, w = unit_grid_lines()
+    tc, arcs = O.TreeCount(n, u, v, w), O.Arcs(n, u, v, w)
+    q = np.array([0, 11, 24 * 11 + 11, 24 * 12 + 12, 300, n - 1], np.int32)
+    half_delta = arcs.bc()[q]
+    pair = tc.rq(q)
+    assert rel_err(tc.bc(arcs)[q], half_delta) <= BC_RTOL
+    assert rel_err(pair, half_delta) > 1e-3  # the wrapped products differ by orders of magnitude
+    n2, u2, v2, w2 = synth.read_graph_lines(os.path.join(GOLDEN, "g2k.txt"))
+    tc2, arcs2 = O.TreeCount(n2, u2, v2, w2), O.Arcs(n2, u2, v2, w2)
+    q2 = np.arange(0, n2, 97, dtype=np.int32)
+    assert rel_err(tc2.rq(q2), arcs2.bc()[q2]) <= BC_RTOL
+

@@ -58,6 +58,64 @@ def test_static_entry_h2h_index():
     assert rel_err(d_bc.cpu().numpy(), idx.bc_sources(np.array([0, 999], np.int32))) <= BC_RTOL
 
 
+def test_static_entry_allocates_no_device_memory():
+    """after a first call (which looks up the array's address), further calls leave the device's
+    free memory and the index's own device bytes unchanged"""
+    import torch
+
+    n, u, v, w = synth.read_graph_lines(os.path.join(GOLDEN, "g2k.txt"))
+    g = Q.Graph(device=0)
+    g.ReadLines(n, u, v, w)
+    idx = g.build_index()
+    d_bc = torch.zeros(n, dtype=torch.float64, device="cuda:0")
+    _static_call(idx, 0, d_bc.data_ptr())
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    bytes0 = int(idx.info()[5])
+    for s in range(1, 40):
+        _static_call(idx, s, d_bc.data_ptr())
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0 and int(idx.info()[5]) == bytes0
+    assert rel_err(d_bc.cpu().numpy(), idx.bc_sources(np.arange(40, dtype=np.int32))) <= BC_RTOL
+
+
+def test_static_entry_csr_index():
+    """the label-free index runs the shortest-path sweep in the static array"""
+    import torch
+
+    n, u, v, w = synth.read_graph_lines(os.path.join(GOLDEN, "g2k.txt"))
+    g = Q.Graph(device=0)
+    g.ReadLines(n, u, v, w)
+    idx = g.build_index(Q.QBC_INDEX_CSR)
+    d_bc = torch.zeros(n, dtype=torch.float64, device="cuda:0")
+    for s in (3, 1500):
+        _static_call(idx, s, d_bc.data_ptr())
+    torch.cuda.synchronize()
+    assert rel_err(d_bc.cpu().numpy(), idx.bc_sources(np.array([3, 1500], np.int32))) <= BC_RTOL
+
+
+def test_static_entry_rejects_trees_taller_than_its_label_kernel():
+    """a 6,000-vertex path has a tree of ~6,000 levels: refused with QBC_EINVAL by the static entry
+    point on a label index, served by the batched path and by the static entry point on a CSR index"""
+    import torch
+
+    n = 6000
+    nn, u, v, w = lines_of([(i, i + 1, 1 + i % 3) for i in range(n - 1)], n)
+    g = Q.Graph(device=0)
+    g.ReadLines(nn, u, v, w)
+    idx = g.build_index()
+    assert int(idx.info()[3]) > 5200
+    d_bc = torch.zeros(n, dtype=torch.float64, device="cuda:0")
+    with pytest.raises(Q.QbcError) as e:
+        _static_call(idx, 0, d_bc.data_ptr())
+    assert e.value.code == capi.QBC_EINVAL and "tree height" in str(e.value)
+    csr = g.build_index(Q.QBC_INDEX_CSR)
+    _static_call(csr, 0, d_bc.data_ptr())
+    torch.cuda.synchronize()
+    assert rel_err(d_bc.cpu().numpy(), csr.bc_sources(np.array([0], np.int32))) <= BC_RTOL
+
+
 def test_static_entry_rejects_graphs_above_the_limit():
     n = 131073  # one more than QBC_STATIC_MAX_VERTICES: a star stays tiny to index
     nn, u, v, w = lines_of([(0, i, 1) for i in range(1, n)], n)
