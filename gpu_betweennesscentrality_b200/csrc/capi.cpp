@@ -278,7 +278,8 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
     if (nparams > 8) need(params[8] >= 0, "label tile must be >= 0");
     if (nparams > 9) need(params[9] >= 0 && params[9] <= 2, "label passes must be 0, 1 or 2");
     if (nparams > 10) need(params[10] >= 0, "sweep bucket width must be >= 0");
-    if (nparams > 11) need(params[11] == 0 || params[11] == 256 || params[11] == 512, "sweep threads must be 0, 256 or 512");
+    if (nparams > 11)
+      need(params[11] == 0 || params[11] == 256 || params[11] == 512 || params[11] == 1024, "sweep threads must be 0, 256, 512 or 1024");
     for (int32_t i = 0; i < nparams && i < kTuningFields; i++) *f[i] = params[i];
     if (nparams > 3 && t.chunk != old_chunk && idx->h.dev) qbc::device_set_chunk(idx->h, t.chunk);
   });

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -60,6 +61,7 @@ struct LabelArgs {
   int32_t multipass;                 // launcher only: rows longer than the tile take several passes
                                      // (kernel variant MP, state in out_rec between passes)
   int32_t *err;                      // device error word (packed kernel's bounded waits)
+  uint32_t wait_spins;               // attempts of a row-copy wait before it is reported
 };
 
 // largest J with lo[J] <= t < hi[J] (entry 0 is the root and always holds), returned as J+1
@@ -259,16 +261,20 @@ __device__ __forceinline__ void bulk_row_to_smem(void *dst, const void *src, uin
                : "memory");
 }
 
-// bounded wait for the phase with the given parity; false when the bound ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (uint32_t it = 0; it < (1u << 22); it++) {
+// Bounded wait of a whole warp for the phase with the given parity: true once every lane has seen
+// the phase complete (each lane's own try_wait is its acquire of the copied row), false when
+// `spins` attempts ran out.  Warp-uniform, so the lanes leave the wait together.
+constexpr uint32_t kRowWaitSpins = 1u << 22;   // a row copy that takes longer is reported
+constexpr uint32_t kDrainWaitSpins = 1u << 28;  // copies still in flight when a CTA gives up
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t spins = kRowWaitSpins) {
+  for (uint32_t it = 0; it < spins; it++) {
     uint32_t ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
         : "r"(smem_addr(bar)), "r"(parity)
         : "memory");
-    if (ok) return true;
+    if (__all_sync(kFull, ok)) return true;
   }
   return false;
 }
@@ -406,7 +412,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
       }
       issue_next();
       const uint32_t b = done % kRowBuffers;
-      if (!mbar_wait(&s_bar[warp][b], (done / kRowBuffers) & 1)) {
+      if (!mbar_wait(&s_bar[warp][b], (done / kRowBuffers) & 1, a.wait_spins)) {
         failed = true;
         break;
       }
@@ -545,10 +551,11 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
     __syncwarp();
   }
   if (failed) {
-    // record, then give the copies still in flight a bounded chance to land before exiting
+    // record, then wait out every copy still in flight into this warp's row buffers before the
+    // CTA's shared memory can be released (the long bound only keeps a broken copy from hanging)
     if (lane == 0 && a.err) atomicCAS(a.err, ERR_NONE, ERR_COPY_TIMEOUT);
     while (done < issued) {
-      mbar_wait(&s_bar[warp][done % kRowBuffers], (done / kRowBuffers) & 1);
+      mbar_wait(&s_bar[warp][done % kRowBuffers], (done / kRowBuffers) & 1, kDrainWaitSpins);
       done++;
     }
     return;
@@ -728,7 +735,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 1) k_label_scan_pair(LabelArg
   };
   auto wait_row = [&](const int32_t *&tbuf) {
     const uint32_t b = done % kPairBuffers;
-    if (!mbar_wait(&s_bar[warp][b], (done / kPairBuffers) & 1)) return false;
+    if (!mbar_wait(&s_bar[warp][b], (done / kPairBuffers) & 1, a.wait_spins)) return false;
     done++;
     tbuf = tb0 + b * S;
     return true;
@@ -878,7 +885,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, 1) k_label_scan_pair(LabelArg
   if (failed) {
     if (lane == 0 && a.err) atomicCAS(a.err, ERR_NONE, ERR_COPY_TIMEOUT);
     while (done < issued) {
-      mbar_wait(&s_bar[warp][done % kPairBuffers], (done / kPairBuffers) & 1);
+      mbar_wait(&s_bar[warp][done % kPairBuffers], (done / kPairBuffers) & 1, kDrainWaitSpins);
       done++;
     }
     return;
@@ -975,6 +982,11 @@ __device__ __forceinline__ int layer_slot(int *ctr, int key) { return atomicAdd(
 __device__ __forceinline__ double rec_rho(const int4 r) { return __hiloint2double(r.w, r.z); }
 __device__ __forceinline__ void set_rho(int4 *r, double x) { reinterpret_cast<double *>(r)[1] = x; }
 
+// A dependency pass leaves at once when the error word is set: the rows it would read come from a
+// label scan or sweep that gave up (its hop layers could index past the layer counters), and the
+// call reports the error anyway.
+__device__ __forceinline__ bool rows_failed(const DepArgs &a) { return a.err && __ldcg(a.err) != ERR_NONE; }
+
 // delta of v, its rho stored in its record, 0.5 * delta added into BC
 template <class RV>
 __device__ __forceinline__ void finish_vertex(const DepArgs &a, const RV &rec, int v, double sv, double sum) {
@@ -988,6 +1000,7 @@ template <class RV>
 __device__ void backprop_levels(const DepArgs &a, const RV &rec, const int32_t *order, const int *start, int maxL);
 
 __global__ void __launch_bounds__(256) k_dependency(DepArgs a) {
+  if (rows_failed(a)) return;
   __shared__ int sh_cnt[kLayerCap + 2];
   __shared__ int sh_cur[kLayerCap + 2];
   __shared__ int red[33];
@@ -1091,6 +1104,7 @@ __device__ __forceinline__ StepIt step_next(const int *cnt, StepIt it, int width
 
 template <bool PIPE>
 __global__ void __launch_bounds__(256, 3) k_dependency_warp(DepArgs a, const int32_t *__restrict__ maxhop, int lcap) {
+  if (rows_failed(a)) return;
   extern __shared__ int smw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const int slot = blockIdx.x * nwarps + warp;
@@ -1352,6 +1366,7 @@ __device__ __forceinline__ void dep_cta_pipe_body(const DepArgs &a, int slot, in
 // The body is instantiated for shared counters (the usual case: shared-memory atomics and loads)
 // and for the per-slot global counters of DAGs deeper than kDepLayerCap layers.
 __global__ void __launch_bounds__(256, 3) k_dependency_cta_pipe(DepArgs a, const int32_t *__restrict__ maxhop) {
+  if (rows_failed(a)) return;
   __shared__ int sh_cnt[kDepLayerCap + 2];
   __shared__ int red[33];
   const int slot = blockIdx.x;
@@ -1366,6 +1381,7 @@ __global__ void __launch_bounds__(256, 3) k_dependency_cta_pipe(DepArgs a, const
 // QBC: sigma by Kahn waves on the SP-DAG from H2H distances (QBC.cu:335-344, :485-555), then
 // the same backprop.  hop[] holds the in-degree until a vertex is queued, then its wave.
 __global__ void __launch_bounds__(256) k_kahn_dependency(DepArgs a) {
+  if (rows_failed(a)) return;
   __shared__ int sh_wave[kLayerCap + 2];
   __shared__ int s_tail, s_flag;
   const int slot = blockIdx.x;
@@ -1618,6 +1634,15 @@ static bool use_packed(const Handle &h, const DeviceState *d, bool plain) {
   return packed_stride(h, d, packed_warps(h, d)) >= 8 && packed_smem(8, 8) <= (size_t)d->smem_optin;
 }
 
+// Attempts of a label-row copy wait before it is reported (ERR_COPY_TIMEOUT).  Test hook: the
+// environment variable QBC_TEST_ROW_WAIT_SPINS overrides it (0: every wait gives up at once), so
+// the timeout path -- error word, drain of the copies in flight, QBC_EDEVICE, recovery -- can be
+// exercised without a slow copy.
+static uint32_t row_wait_spins() {
+  const char *e = std::getenv("QBC_TEST_ROW_WAIT_SPINS");
+  return e && *e ? (uint32_t)std::strtoul(e, nullptr, 10) : kRowWaitSpins;
+}
+
 static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t *src, int32_t ns, bool plain,
                          cudaStream_t st) {
   if (h.host.kind == IndexKind::CSR) {  // no labels: shortest-path sweeps give the rows
@@ -1657,6 +1682,7 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t
   a.aend = d->aend;
   a.bits = d->packed_bits;
   a.err = d->err;
+  a.wait_spins = row_wait_spins();
   const int groups = (ns + p.G - 1) / p.G;
   CK(cudaMemsetAsync(d->maxhop[buf], 0, (size_t)ns * 4, st));
   std::pair<cudaEvent_t, cudaEvent_t> ev{};
@@ -2520,6 +2546,7 @@ void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *s
     la.split = p.split;
     la.out_rec = rec;
     la.out_hop = hop;
+    la.wait_spins = kRowWaitSpins;
     if (h.host.kind == IndexKind::MHL) launch_label_c<true>(p, la, 1, st);
     else launch_label_c<false>(p, la, 1, st);
   }

@@ -21,7 +21,7 @@ struct Tuning {
   int32_t label_tile = 0;        // label entries per row staged in shared memory; 0 = all that fit
   int32_t label_passes = 0;      // rows longer than the tile: 0/1 one pass + global tail, 2 several tile passes
   int32_t sweep_delta = 0;       // CSR index: distance bucket width of the shortest-path sweep; 0 = auto
-  int32_t sweep_threads = 0;     // CSR index: threads per CTA of the sweep (256 or 512; 0 = 512)
+  int32_t sweep_threads = 0;     // CSR index: threads per CTA of the sweep (256, 512 or 1024; 0 = 512)
 };
 
 struct DeviceState;  // opaque, defined in device_state.h

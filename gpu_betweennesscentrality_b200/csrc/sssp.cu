@@ -310,7 +310,7 @@ __device__ __forceinline__ void relax_grid(int4 *rec, int u, int nd, int T, int 
 
 // rec/hop/order/lcnt: the single slot of a one-source buffer (plain rows); far lists ping-pong
 // between the second half of the layer-counter row and the hop row (written only by the waves)
-__global__ void __launch_bounds__(512) k_sweep_rows_grid(SweepArgs a, GridCtl *c) {
+__global__ void __launch_bounds__(1024) k_sweep_rows_grid(SweepArgs a, GridCtl *c) {
   const int s = a.src[0];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   int4 *rec = a.rec;
@@ -461,6 +461,7 @@ void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop,
   a.maxhop = maxhop;
   a.err = d->err;
   if (h.tuning.sweep_threads == 256) k_sweep_rows<256><<<ns, 256, 0, st>>>(a);
+  else if (h.tuning.sweep_threads == 1024) k_sweep_rows<1024><<<ns, 1024, 0, st>>>(a);
   else k_sweep_rows<512><<<ns, 512, 0, st>>>(a);
   CK(cudaGetLastError());
 }
@@ -483,15 +484,16 @@ void launch_sweep_rows_grid(const Handle &h, DeviceState *d, int4 *rec, int32_t 
   a.lcnt = lcnt;
   a.maxhop = nullptr;
   a.err = d->err;
-  // every CTA of the grid resident at once (the barrier waits on all of them)
+  // one 1,024-thread CTA per SM, all resident at once (the barrier waits on every one of them;
+  // fewer, larger CTAs make each barrier cheaper)
   int per_sm = 0, sms = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_rows_grid, 512, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_rows_grid, 1024, 0));
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device));
   if (per_sm < 1) throw Error(QBC_EDEVICE, "plain sweep kernel does not fit an SM");
   GridCtl *c = reinterpret_cast<GridCtl *>(d->grid_ctl);
   CK(cudaMemsetAsync(c, 0, sizeof(GridCtl), st));
   void *args[] = {&a, &c};
-  CK(cudaLaunchCooperativeKernel((const void *)k_sweep_rows_grid, dim3((unsigned)(per_sm * sms)), dim3(512), args, 0, st));
+  CK(cudaLaunchCooperativeKernel((const void *)k_sweep_rows_grid, dim3((unsigned)sms), dim3(1024), args, 0, st));
 }
 
 }  // namespace qbc

@@ -126,7 +126,7 @@ int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int3
  * rows longer than the tile (0 = 1: one launch, entries beyond the tile read from global memory;
  * 2: one launch per tile of entries, the pairs' running minima kept in the output rows between
  * passes), [10]=distance bucket width of the CSR index's shortest-path sweep (0 = auto: twice the
- * mean arc weight), [11]=threads per CTA of that sweep (256 or 512; 0 = 512).  Refused with
+ * mean arc weight), [11]=threads per CTA of that sweep (256, 512 or 1024; 0 = 512).  Refused with
  * QBC_EBUSY while the index serves. */
 int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams);
 int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams);

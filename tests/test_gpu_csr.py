@@ -71,7 +71,8 @@ def test_rows_and_full_bc_shortcut_graphs(n_target, seed, sc):
     assert rel_err(idx.bc_all(), arcs.bc()) <= BC_RTOL
 
 
-@pytest.mark.parametrize("delta,threads", [(1, 256), (37, 512), (1000, 256), (1 << 20, 512), (0, 512)])
+@pytest.mark.parametrize("delta,threads", [(1, 256), (37, 512), (1000, 256), (1 << 20, 512), (0, 512), (0, 1024),
+                                           (1, 1024)])
 def test_bucket_widths_and_threads_give_identical_rows(delta, threads):
     """bucket width 1 (label-setting), the default, and one bucket holding every distance
     (Bellman-Ford on the whole graph) all reach the same fixed point"""

@@ -9,7 +9,7 @@ import pytest
 import gpu_betweennesscentrality_b200 as Q
 import pyoracle as O
 from conftest import GOLDEN, ROOT, rel_err
-from gpu_betweennesscentrality_b200 import synth
+from gpu_betweennesscentrality_b200 import capi, synth
 from util import BC_RTOL, KNOWN, grid_lines, lines_of, unit_grid_lines
 
 pytestmark = pytest.mark.gpu
@@ -296,6 +296,27 @@ def test_la_full_bc_matches_reference_gpu(la_path):
     if os.path.exists(p):
         assert rel_err(bc, np.load(p)["bc"]) <= BC_RTOL
     assert rel_err(idx.bc_sources(srcs), tc.bc(O.Arcs(n, u, v, w), srcs)) <= BC_RTOL
+
+
+def test_row_copy_wait_timeout_is_reported_and_the_index_recovers(g2k):
+    """A label-row copy wait that runs out sets the error word; the warp waits out its copies in
+    flight, the dependency pass skips the partial rows, the call returns QBC_EDEVICE, and the next
+    call on the same index is correct.  QBC_TEST_ROW_WAIT_SPINS=0 makes every wait give up at once."""
+    n, u, v, w, g, idx, tc, arcs = g2k
+    srcs = np.arange(0, n, 7, dtype=np.int32)
+    ref = idx.bc_sources(srcs)
+    os.environ["QBC_TEST_ROW_WAIT_SPINS"] = "0"
+    try:
+        with pytest.raises(Q.QbcError) as e:
+            idx.bc_sources(srcs)
+        assert e.value.code == capi.QBC_EDEVICE and "copy wait" in str(e.value)
+    finally:
+        del os.environ["QBC_TEST_ROW_WAIT_SPINS"]
+    assert rel_err(idx.bc_sources(srcs), ref) <= BC_RTOL
+    d, c, h = idx.rows(srcs[:5])
+    for k, s_ in enumerate(srcs[:5]):
+        d0, c0, h0 = tc.rows(int(s_))
+        assert np.array_equal(d[k], d0) and np.array_equal(c[k], c0) and np.array_equal(h[k], h0)
 
 
 def test_errors_are_reported(g2k):
