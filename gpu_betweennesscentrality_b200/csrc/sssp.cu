@@ -99,8 +99,30 @@ __device__ __forceinline__ void for_arcs(const SweepArgs &a, int v, F &&f) {
   }
 }
 
+// The first four arcs of v as (head, weight) pairs, head -1 where absent; *rest = the range of
+// further arcs in arc_hw (empty for at most four arcs).  A visit loads all four heads' records
+// before it issues any atomic: a load after an atomic cannot be moved above it (the addresses
+// might alias), so checking the arcs one by one made each visit wait for four DRAM round trips.
+struct Arcs4 {
+  int h[4], w[4];
+  int rest_b, rest_e;
+};
+__device__ __forceinline__ Arcs4 arcs4(const SweepArgs &a, int v) {
+  const int4 p0 = __ldg(a.arc4 + 2 * v), p1 = __ldg(a.arc4 + 2 * v + 1);
+  Arcs4 r;
+  r.h[0] = p0.x; r.w[0] = p0.y;
+  r.h[1] = p0.z; r.w[1] = p0.w;
+  r.h[2] = p1.x; r.w[2] = p1.y;
+  const bool more = p1.z < -1;
+  r.h[3] = more ? -1 : p1.z;
+  r.w[3] = p1.w;
+  r.rest_b = more ? ~p1.z : 0;
+  r.rest_e = more ? p1.w : 0;
+  return r;
+}
+
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) k_sweep_rows(SweepArgs a) {
+__global__ void __launch_bounds__(THREADS, 2048 / THREADS) k_sweep_rows(SweepArgs a) {
   __shared__ SweepShared sh;
   const int slot = blockIdx.x;
   if (slot >= a.ns) return;
@@ -135,7 +157,17 @@ __global__ void __launch_bounds__(THREADS) k_sweep_rows(SweepArgs a) {
       for (int i = tid; i < len; i += THREADS) {
         const int v = near[i];
         const int dv = rec[v].x;
-        for_arcs(a, v, [&](int u, int w) { relax(rec, u, dv + w, T, pass, far_tag, next, far, sh); });
+        const Arcs4 q = arcs4(a, v);
+        int du[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) du[k] = q.h[k] >= 0 ? rec[q.h[k]].x : INT_MIN;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          if (dv + q.w[k] < du[k]) relax(rec, q.h[k], dv + q.w[k], T, pass, far_tag, next, far, sh);
+        for (int e = q.rest_b; e < q.rest_e; e++) {
+          const int2 hw = __ldg(a.arc_hw + e);
+          relax(rec, hw.x, dv + hw.y, T, pass, far_tag, next, far, sh);
+        }
       }
       __syncthreads();
       if (tid == 0) {
@@ -226,12 +258,22 @@ __global__ void __launch_bounds__(THREADS) k_sweep_rows(SweepArgs a) {
       const int v = queue[i];
       const int4 r = rec[v];
       hop[v] = L;
-      for_arcs(a, v, [&](int h, int w) {
+      auto push = [&](int h) {
         int4 &rh = rec[h];
-        if (rh.x != r.x + w) return;
         atomicAdd(&rh.y, r.y);                                            // 32-bit wrapping, as count_t
         if (atomicSub(&rh.z, 1) == 1) queue[atomicAdd(&sh.tail, 1)] = h;  // its last predecessor
-      });
+      };
+      const Arcs4 q = arcs4(a, v);
+      int dh[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) dh[k] = q.h[k] >= 0 ? rec[q.h[k]].x : INT_MIN;
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        if (dh[k] == r.x + q.w[k]) push(q.h[k]);
+      for (int x = q.rest_b; x < q.rest_e; x++) {
+        const int2 hw = __ldg(a.arc_hw + x);
+        if (rec[hw.x].x == r.x + hw.y) push(hw.x);
+      }
     }
     __syncthreads();
     b = e;
@@ -310,7 +352,7 @@ __device__ __forceinline__ void relax_grid(int4 *rec, int u, int nd, int T, int 
 
 // rec/hop/order/lcnt: the single slot of a one-source buffer (plain rows); far lists ping-pong
 // between the second half of the layer-counter row and the hop row (written only by the waves)
-__global__ void __launch_bounds__(1024) k_sweep_rows_grid(SweepArgs a, GridCtl *c) {
+__global__ void __launch_bounds__(1024, 1) k_sweep_rows_grid(SweepArgs a, GridCtl *c) {
   const int s = a.src[0];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   int4 *rec = a.rec;
@@ -336,7 +378,17 @@ __global__ void __launch_bounds__(1024) k_sweep_rows_grid(SweepArgs a, GridCtl *
       for (int i = gt; i < len; i += gs) {
         const int v = ldcg(near + i);
         const int dv = ldcg(reinterpret_cast<const int *>(rec + v));
-        for_arcs(a, v, [&](int u, int w) { relax_grid(rec, u, dv + w, T, pass, far_tag, next, far, c); });
+        const Arcs4 q = arcs4(a, v);
+        int du[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) du[k] = q.h[k] >= 0 ? ldcg(reinterpret_cast<const int *>(rec + q.h[k])) : INT_MIN;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          if (dv + q.w[k] < du[k]) relax_grid(rec, q.h[k], dv + q.w[k], T, pass, far_tag, next, far, c);
+        for (int e = q.rest_b; e < q.rest_e; e++) {
+          const int2 hw = __ldg(a.arc_hw + e);
+          relax_grid(rec, hw.x, dv + hw.y, T, pass, far_tag, next, far, c);
+        }
       }
       if (!grid_sync(c, gen, a.err)) return;
       if (gt == 0) {
@@ -417,12 +469,22 @@ __global__ void __launch_bounds__(1024) k_sweep_rows_grid(SweepArgs a, GridCtl *
       const int dv = ldcg(reinterpret_cast<const int *>(rec + v));
       const int sv = ldcg(reinterpret_cast<const int *>(rec + v) + 1);
       a.hop[v] = L;
-      for_arcs(a, v, [&](int h, int w) {
+      auto push = [&](int h) {
         int *rh = reinterpret_cast<int *>(rec + h);
-        if (ldcg(rh) != dv + w) return;
         atomicAdd(rh + 1, sv);
         if (atomicSub(rh + 2, 1) == 1) queue[atomicAdd(&c->tail, 1)] = h;
-      });
+      };
+      const Arcs4 q = arcs4(a, v);
+      int dh[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) dh[k] = q.h[k] >= 0 ? ldcg(reinterpret_cast<const int *>(rec + q.h[k])) : INT_MIN;
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        if (dh[k] == dv + q.w[k]) push(q.h[k]);
+      for (int x = q.rest_b; x < q.rest_e; x++) {
+        const int2 hw = __ldg(a.arc_hw + x);
+        if (ldcg(reinterpret_cast<const int *>(rec + hw.x)) == dv + hw.y) push(hw.x);
+      }
     }
     if (!grid_sync(c, gen, a.err)) return;
     b = e;
