@@ -59,7 +59,69 @@ struct SweepArgs {
   int32_t *lcnt;       // [ns][2 (n_pad + 2)]: next near list, far list
   int32_t *maxhop;     // [ns] largest hop layer per source, or null
   int32_t *err;
+  int32_t sort_shift;    // frontier lists are visited in order of v >> sort_shift ...
+  int32_t sort_buckets;  // ... (n_pad - 1) >> sort_shift < sort_buckets <= kSortBuckets
 };
+
+constexpr int kSortBuckets = 4096;  // shared-memory counters of the frontier ordering
+constexpr int kSortMinLen = 1024;   // shorter lists are visited as they are
+
+// Exclusive scan of c[0..len) in place (len <= kSortBuckets), whole CTA; red holds 33 ints.
+template <int THREADS>
+__device__ __forceinline__ void cta_exclusive_scan(int *c, int len, int *red) {
+  constexpr int per = (kSortBuckets + THREADS - 1) / THREADS;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int b = tid * per;
+  int local = 0;
+#pragma unroll
+  for (int k = 0; k < per; k++) local += (b + k < len) ? c[b + k] : 0;
+  int x = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kSweepFull, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) red[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int t = lane < THREADS / 32 ? red[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kSweepFull, t, o);
+      if (lane >= o) t += y;
+    }
+    red[lane] = t;  // inclusive warp totals
+  }
+  __syncthreads();
+  int run = x - local + (warp > 0 ? red[warp - 1] : 0);
+#pragma unroll
+  for (int k = 0; k < per; k++)
+    if (b + k < len) {
+      const int v = c[b + k];
+      c[b + k] = run;
+      run += v;
+    }
+  __syncthreads();
+}
+
+// Frontier ordering: a list of vertices is rewritten into `out` grouped by v >> shift (a counting
+// sort, CTA-wide), so that a pass visits the frontier in vertex-id order.  Near lists and Kahn
+// waves are bands of the graph; in id order consecutive visits share record lines, and the rows
+// above and below are visited soon after, while their lines are still in L1/L2.
+template <int THREADS, class IN, class OUT>
+__device__ __forceinline__ void order_frontier(const SweepArgs &a, IN in, int len, OUT out, int *hist, int *red) {
+  const int tid = threadIdx.x;
+  for (int i = tid; i < a.sort_buckets; i += THREADS) hist[i] = 0;
+  __syncthreads();
+  for (int i = tid; i < len; i += THREADS) atomicAdd(hist + (in(i) >> a.sort_shift), 1);
+  __syncthreads();
+  cta_exclusive_scan<THREADS>(hist, a.sort_buckets, red);
+  for (int i = tid; i < len; i += THREADS) {
+    const int v = in(i);
+    out(atomicAdd(hist + (v >> a.sort_shift), 1)) = v;
+  }
+  __syncthreads();
+}
 
 // Shared state of one CTA's sweep.  Record field y while sweeping: > 0 the pass whose next list
 // holds the vertex; < 0 the (negated, minus one) far-list split round whose far list holds it; 0
@@ -122,8 +184,10 @@ __device__ __forceinline__ Arcs4 arcs4(const SweepArgs &a, int v) {
 }
 
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, 2048 / THREADS) k_sweep_rows(SweepArgs a) {
+__global__ void __launch_bounds__(THREADS, 1536 / THREADS) k_sweep_rows(SweepArgs a) {
   __shared__ SweepShared sh;
+  __shared__ int hist[kSortBuckets];
+  __shared__ int red[33];
   const int slot = blockIdx.x;
   if (slot >= a.ns) return;
   const int s = a.src[slot];
@@ -154,8 +218,13 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) k_sweep_rows(SweepArg
         break;
       }
       const int far_tag = -1 - round;
+      // a long list is visited in vertex-id order, staged in the hop row (free until the waves)
+      const bool sorted = len >= kSortMinLen;
+      if (sorted)
+        order_frontier<THREADS>(
+            a, [&](int i) { return near[i]; }, len, [&](int i) -> int32_t & { return hop[i]; }, hist, red);
       for (int i = tid; i < len; i += THREADS) {
-        const int v = near[i];
+        const int v = sorted ? hop[i] : near[i];
         const int dv = rec[v].x;
         const Arcs4 q = arcs4(a, v);
         int du[4];
@@ -253,9 +322,15 @@ __global__ void __launch_bounds__(THREADS, 2048 / THREADS) k_sweep_rows(SweepArg
   }
   __syncthreads();
   int L = 0, b = 0, e = 1;
+  int32_t *wave = a.lcnt + (size_t)slot * 2 * (a.n_pad + 2);  // the next-list row is free now
   while (b < e) {
+    // a long wave is visited in vertex-id order, staged in the next-list row
+    const bool sorted = e - b >= kSortMinLen;
+    if (sorted)
+      order_frontier<THREADS>(
+          a, [&](int i) { return queue[b + i]; }, e - b, [&](int i) -> int32_t & { return wave[i]; }, hist, red);
     for (int i = b + tid; i < e; i += THREADS) {
-      const int v = queue[i];
+      const int v = sorted ? wave[i - b] : queue[i];
       const int4 r = rec[v];
       hop[v] = L;
       auto push = [&](int h) {
@@ -522,6 +597,9 @@ void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop,
   a.lcnt = lcnt;
   a.maxhop = maxhop;
   a.err = d->err;
+  a.sort_shift = 0;
+  while (((d->n_pad - 1) >> a.sort_shift) >= kSortBuckets) a.sort_shift++;
+  a.sort_buckets = ((d->n_pad - 1) >> a.sort_shift) + 1;
   if (h.tuning.sweep_threads == 256) k_sweep_rows<256><<<ns, 256, 0, st>>>(a);
   else if (h.tuning.sweep_threads == 1024) k_sweep_rows<1024><<<ns, 1024, 0, st>>>(a);
   else k_sweep_rows<512><<<ns, 512, 0, st>>>(a);
