@@ -909,6 +909,10 @@ struct DepArgs {
   int32_t *lcnt;   // [ns][2*(n_pad+2)] global layer counters when shared ones do not suffice
   double *bc;      // [n] tid order, FP64 red target
   int32_t *err;
+  // records carry DAG-successor masks in their last word until rho overwrites it (the label-free
+  // sweep writes them: bit k for the k-th of the first four arcs, bit 4 for a later arc), so the
+  // pipelined backprop loads only successors' records; 0 = every arc is checked
+  int32_t succ_mask;
 };
 
 __device__ __forceinline__ int block_reduce_max(int v, int *red) {
@@ -1332,15 +1336,16 @@ __device__ __forceinline__ void dep_cta_pipe_body(const DepArgs &a, int slot, in
     const int vN = vertex_at(itN);
     if (vC >= 0) {
       const int hd[4] = {aC0.x, aC0.z, aC1.x, aC1.z}, wt[4] = {aC0.y, aC0.w, aC1.y, aC1.w};
+      const int msk = a.succ_mask ? rC.w : 0x1f;  // own record: still the mask, rho comes below
       int4 rw[4];
 #pragma unroll
       for (int q = 0; q < 4; q++)
-        if (hd[q] >= 0) rw[q] = rec[hd[q]];
+        if (hd[q] >= 0 && ((msk >> q) & 1)) rw[q] = rec[hd[q]];
       double acc = 0.0;
 #pragma unroll
       for (int q = 0; q < 4; q++)
-        if (hd[q] >= 0 && rw[q].x == rC.x + wt[q]) acc += rec_rho(rw[q]);
-      if (hd[3] < -1) {  // arcs beyond the third, in arc order
+        if (hd[q] >= 0 && ((msk >> q) & 1) && rw[q].x == rC.x + wt[q]) acc += rec_rho(rw[q]);
+      if (hd[3] < -1 && (msk & 16)) {  // arcs beyond the third, in arc order
         for (int e = ~hd[3]; e < wt[3]; e++) {
           const int2 hw = __ldcg(a.arc_hw + e);
           const int4 r = rec[hw.x];
@@ -1754,6 +1759,7 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *
       k_dependency_warp<true><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
     else k_dependency_warp<false><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
   } else if (counted && form == 4 && !plain) {
+    a.succ_mask = h.host.kind == IndexKind::CSR ? 1 : 0;  // the sweep's records carry successor masks
     k_dependency_cta_pipe<<<ns, threads, 0, st>>>(a, d->maxhop[buf]);
   } else if (counted) {
     k_dependency<<<ns, threads, 0, st>>>(a);

@@ -308,12 +308,29 @@ __global__ void __launch_bounds__(THREADS, 1536 / THREADS) k_sweep_rows(SweepArg
     return;
   }
   // ---- counts and hop layers: in-degrees over the DAG (vertex order: neighbours' records are
-  // mostly in the same or the next sectors), record (dist, count = [v == s], in-degree, 0)
+  // mostly in the same or the next sectors), record (dist, count = [v == s], in-degree, successor
+  // mask).  The same neighbour distances give the DAG successors (d[h] == d[v] + w): bit k of the
+  // mask for the first four arcs, bit 4 when a further arc is one, so a wave visit touches only its
+  // successors' records instead of gathering every neighbour's distance.
   for (int v = tid; v < a.n; v += THREADS) {
     const int dv = rec[v].x;
-    int c = 0;
-    for_arcs(a, v, [&](int h, int w) { c += rec[h].x + w == dv; });
-    rec[v] = make_int4(dv, v == s ? 1 : 0, c, 0);
+    const Arcs4 q = arcs4(a, v);
+    int dh[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) dh[k] = q.h[k] >= 0 ? rec[q.h[k]].x : INT_MIN;
+    int c = 0, m = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      c += q.h[k] >= 0 && dh[k] + q.w[k] == dv;
+      m |= (q.h[k] >= 0 && dh[k] == dv + q.w[k]) << k;
+    }
+    for (int e = q.rest_b; e < q.rest_e; e++) {
+      const int2 hw = __ldg(a.arc_hw + e);
+      const int dx = rec[hw.x].x;
+      c += dx + hw.y == dv;
+      m |= (dx == dv + hw.y) << 4;
+    }
+    rec[v] = make_int4(dv, v == s ? 1 : 0, c, m);
   }
   int32_t *queue = a.order + (size_t)slot * a.n_pad;
   if (tid == 0) {
@@ -339,16 +356,14 @@ __global__ void __launch_bounds__(THREADS, 1536 / THREADS) k_sweep_rows(SweepArg
         if (atomicSub(&rh.z, 1) == 1) queue[atomicAdd(&sh.tail, 1)] = h;  // its last predecessor
       };
       const Arcs4 q = arcs4(a, v);
-      int dh[4];
-#pragma unroll
-      for (int k = 0; k < 4; k++) dh[k] = q.h[k] >= 0 ? rec[q.h[k]].x : INT_MIN;
 #pragma unroll
       for (int k = 0; k < 4; k++)
-        if (dh[k] == r.x + q.w[k]) push(q.h[k]);
-      for (int x = q.rest_b; x < q.rest_e; x++) {
-        const int2 hw = __ldg(a.arc_hw + x);
-        if (rec[hw.x].x == r.x + hw.y) push(hw.x);
-      }
+        if ((r.w >> k) & 1) push(q.h[k]);
+      if (r.w & 16)
+        for (int x = q.rest_b; x < q.rest_e; x++) {
+          const int2 hw = __ldg(a.arc_hw + x);
+          if (rec[hw.x].x == r.x + hw.y) push(hw.x);
+        }
     }
     __syncthreads();
     b = e;
