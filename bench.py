@@ -394,7 +394,7 @@ def config_shortcuts_1m(q, args, dev, flush, peak, peak_src):
     tune = None
     if not args.no_autotune:
         t = time.perf_counter()
-        tune = idx.autotune(sample[:512])
+        tune = idx.autotune(sample)  # the step's own sample: chunk and occupancy as timed
         tune["seconds"] = round(time.perf_counter() - t, 2)
     steps = min(args.steps, 5)
     clocks = ClockSampler(dev.index or 0).start()
