@@ -909,11 +909,10 @@ struct DepArgs {
   int32_t *lcnt;   // [ns][2*(n_pad+2)] global layer counters when shared ones do not suffice
   double *bc;      // [n] tid order, FP64 red target
   int32_t *err;
-  // records carry DAG-successor masks in their last word until rho overwrites it (the label-free
-  // sweep writes them: bit k for the k-th of the first four arcs, bit 4 for a later arc), so the
-  // pipelined backprop loads only successors' records; 0 = every arc is checked
-  int32_t succ_mask;
 };
+// The label-free sweep's records carry DAG-successor masks in their last word until rho overwrites
+// it (bit k for the k-th of the first four arcs, bit 4 for a later arc); k_dependency_cta_pipe<true>
+// loads only those successors' records.
 
 __device__ __forceinline__ int block_reduce_max(int v, int *red) {
   v = __reduce_max_sync(kFull, v);
@@ -1275,7 +1274,7 @@ __global__ void __launch_bounds__(256, 3) k_dependency_warp(DepArgs a, const int
 // reads layer L as [cnt[L - 1], cnt[L]) through the pointer cnt - 1.
 constexpr int kDepLayerCap = 2046;
 
-template <class CNT>
+template <bool MASK, class CNT>
 __device__ __forceinline__ void dep_cta_pipe_body(const DepArgs &a, int slot, int maxL, CNT *cnt, int *red) {
   const int s = a.src[slot];
   const size_t base = (size_t)slot * a.n_pad;
@@ -1336,7 +1335,7 @@ __device__ __forceinline__ void dep_cta_pipe_body(const DepArgs &a, int slot, in
     const int vN = vertex_at(itN);
     if (vC >= 0) {
       const int hd[4] = {aC0.x, aC0.z, aC1.x, aC1.z}, wt[4] = {aC0.y, aC0.w, aC1.y, aC1.w};
-      const int msk = a.succ_mask ? rC.w : 0x1f;  // own record: still the mask, rho comes below
+      const int msk = MASK ? rC.w : 0x1f;  // own record: still the mask, rho comes below
       int4 rw[4];
 #pragma unroll
       for (int q = 0; q < 4; q++)
@@ -1369,7 +1368,9 @@ __device__ __forceinline__ void dep_cta_pipe_body(const DepArgs &a, int slot, in
 }
 
 // The body is instantiated for shared counters (the usual case: shared-memory atomics and loads)
-// and for the per-slot global counters of DAGs deeper than kDepLayerCap layers.
+// and for the per-slot global counters of DAGs deeper than kDepLayerCap layers; MASK for records
+// that carry DAG-successor masks (the label-free sweep's), so the label path's code has no mask test.
+template <bool MASK>
 __global__ void __launch_bounds__(256, 3) k_dependency_cta_pipe(DepArgs a, const int32_t *__restrict__ maxhop) {
   if (rows_failed(a)) return;
   __shared__ int sh_cnt[kDepLayerCap + 2];
@@ -1378,9 +1379,9 @@ __global__ void __launch_bounds__(256, 3) k_dependency_cta_pipe(DepArgs a, const
   if (slot >= a.ns) return;
   const int maxL = maxhop[slot];
   if (maxL <= kDepLayerCap)
-    dep_cta_pipe_body(a, slot, maxL, sh_cnt, red);
+    dep_cta_pipe_body<MASK>(a, slot, maxL, sh_cnt, red);
   else
-    dep_cta_pipe_body(a, slot, maxL, a.lcnt + (size_t)slot * 2 * (a.n_pad + 2), red);
+    dep_cta_pipe_body<MASK>(a, slot, maxL, a.lcnt + (size_t)slot * 2 * (a.n_pad + 2), red);
 }
 
 // QBC: sigma by Kahn waves on the SP-DAG from H2H distances (QBC.cu:335-344, :485-555), then
@@ -1759,8 +1760,10 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *
       k_dependency_warp<true><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
     else k_dependency_warp<false><<<(ns + wpb - 1) / wpb, wpb * 32, smem, st>>>(a, d->maxhop[buf], lcap);
   } else if (counted && form == 4 && !plain) {
-    a.succ_mask = h.host.kind == IndexKind::CSR ? 1 : 0;  // the sweep's records carry successor masks
-    k_dependency_cta_pipe<<<ns, threads, 0, st>>>(a, d->maxhop[buf]);
+    if (h.host.kind == IndexKind::CSR)  // the sweep's records carry successor masks
+      k_dependency_cta_pipe<true><<<ns, threads, 0, st>>>(a, d->maxhop[buf]);
+    else
+      k_dependency_cta_pipe<false><<<ns, threads, 0, st>>>(a, d->maxhop[buf]);
   } else if (counted) {
     k_dependency<<<ns, threads, 0, st>>>(a);
   } else {
@@ -2050,7 +2053,8 @@ static DeviceState *new_state(Handle &h, int device) {
   // the dependency pass wants L1, not shared memory: 3 CTAs x 9.5 KB fit the 32 KB carveout
   // (14 % of 228 KB), which leaves 224 KB of L1 instead of the 192 KB the driver picks by itself
   // (76.6 vs 78.8 ms per all-source step at 50k)
-  CK(cudaFuncSetAttribute(k_dependency_cta_pipe, cudaFuncAttributePreferredSharedMemoryCarveout, 14));
+  CK(cudaFuncSetAttribute(k_dependency_cta_pipe<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 14));
+  CK(cudaFuncSetAttribute(k_dependency_cta_pipe<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 14));
   d->n = ix.n;
   d->n_pad = (ix.n + 7) & ~7;
   int S = (ix.tree_height + 3) & ~3;
