@@ -43,10 +43,11 @@ constexpr unsigned kFull = 0xffffffffu;
 
 // ------------------------------------------------------------------------------- K1 + K2
 struct LabelArgs {
+  // label distances, shifted left by `bits` when the packed-key kernel applies (one array serves
+  // both kernels: the general one shifts back as it loads)
   const int32_t *__restrict__ dis;
-  const int32_t *__restrict__ dis_sh;  // dis << bits (packed kernel: keys and target rows pre-shifted)
+  const int32_t *__restrict__ dis_sh;  // the same array (packed kernel: keys and target rows pre-shifted)
   const int2 *__restrict__ ch;
-  const int32_t *__restrict__ anc;
   const int64_t *__restrict__ lab_off;
   const int32_t *__restrict__ depth;
   const int32_t *__restrict__ send;
@@ -55,7 +56,10 @@ struct LabelArgs {
   int4 *__restrict__ out_rec;     // [ns][n_pad] records (dist, count bits, delta as f64 = 0)
   int32_t *__restrict__ out_hop;  // [ns][n_pad]
   int32_t *__restrict__ maxhop;   // [ns] largest hop layer per source (atomicMax), or null
-  const int32_t *__restrict__ aend;  // subtree end of each row entry's ancestor (packed kernel)
+  // per slot of the launch: the source's ancestor ids (root first), then their subtree ends, each
+  // row `src_stride` ints (k_src_rows writes them from the parent links before the scan)
+  const int32_t *__restrict__ src_rows;
+  int32_t src_stride;
   int32_t bits;                      // index bits of the packed keys (packed kernel)
   int32_t pass_lo;                   // multi-pass packed kernel: first row entry of this pass's tile
   int32_t multipass;                 // launcher only: rows longer than the tile take several passes
@@ -105,9 +109,10 @@ __global__ void __launch_bounds__(256, 1) k_label_scan(LabelArgs a) {
     const int i = idx / S, j = idx - i * S;
     int vd = 0x3fffffff, vlo = INT_MAX, vhi = -1;
     if (i < gcount && j < s_h[i]) {
-      vd = a.dis[s_off[i] + j];
-      vlo = a.anc[s_off[i] + j];
-      vhi = a.send[vlo];
+      const int32_t *row = a.src_rows + (size_t)(first + i) * 2 * a.src_stride;
+      vd = (int)((uint32_t)a.dis[s_off[i] + j] >> a.bits);
+      vlo = row[j];
+      vhi = row[a.src_stride + j];
     }
     s_dis[idx] = vd;
     s_lo[idx] = vlo;
@@ -137,8 +142,14 @@ __global__ void __launch_bounds__(256, 1) k_label_scan(LabelArgs a) {
         const int64_t toff = a.lab_off[t];
         const int hl = have ? lca_depth(slo, shi, hs, t) : 0;
         const int H = __reduce_max_sync(kFull, hl);
-        for (int j = lane * 4; j < H; j += 128)
-          *reinterpret_cast<int4 *>(tbuf + j) = __ldg(reinterpret_cast<const int4 *>(a.dis + toff + j));
+        for (int j = lane * 4; j < H; j += 128) {
+          int4 x = __ldg(reinterpret_cast<const int4 *>(a.dis + toff + j));
+          x.x = (int)((uint32_t)x.x >> a.bits);
+          x.y = (int)((uint32_t)x.y >> a.bits);
+          x.z = (int)((uint32_t)x.z >> a.bits);
+          x.w = (int)((uint32_t)x.w >> a.bits);
+          *reinterpret_cast<int4 *>(tbuf + j) = x;
+        }
         __syncwarp();
         if (K == 1) {
           int m = INT_MAX, jm = 0;
@@ -339,8 +350,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
   const int hs = have ? s_h[lane] : 1;
   const int64_t soff = s_off[lane];
   const uint32_t *srow = s_key + lane * S;
-  const int32_t *lo = a.anc + soff;
-  const int32_t *hi = a.aend + soff;
+  const int32_t *lo = a.src_rows + (size_t)(first + (have ? lane : 0)) * 2 * a.src_stride;
+  const int32_t *hi = lo + a.src_stride;
   const int nsteps = 32 - __clz(hs);
   int mh = 0;
   bool failed = false;
@@ -710,8 +721,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, 1) k_label_scan_pair(LabelArg
   const int hs = have ? s_h[lane] : 1;
   const int64_t soff = s_off[lane];
   const uint32_t *srow = s_key + lane * S;
-  const int32_t *lo = a.anc + soff;
-  const int32_t *hi = a.aend + soff;
+  const int32_t *lo = a.src_rows + (size_t)(first + (have ? lane : 0)) * 2 * a.src_stride;
+  const int32_t *hi = lo + a.src_stride;
   const int nsteps = 32 - __clz(hs);
   int mh = 0;
   bool failed = false;
@@ -1469,6 +1480,24 @@ __global__ void __launch_bounds__(256) k_kahn_dependency(DepArgs a) {
   backprop_levels(a, rec, order, wave, L - 1);
 }
 
+// Each slot's source: its ancestors root first (the tree path, walked up from the source by parent
+// links) and their subtree ends -- the nested intervals the label kernels test targets against,
+// derived per launch instead of stored for every label entry (4 + 4 bytes per entry saved).
+__global__ void k_src_rows(const int32_t *__restrict__ src, int32_t ns, const int32_t *__restrict__ depth,
+                           const int32_t *__restrict__ parent, const int32_t *__restrict__ send, int32_t stride,
+                           int32_t *__restrict__ rows) {
+  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < ns; slot += gridDim.x * blockDim.x) {
+    const int s = src[slot];
+    int32_t *lo = rows + (size_t)slot * 2 * stride, *hi = lo + stride;
+    int x = s;
+    for (int j = depth[s] - 1; j >= 0; j--) {
+      lo[j] = x;
+      hi[j] = send[x];
+      x = parent[x];
+    }
+  }
+}
+
 __global__ void k_tid_to_vid_f64(const double *__restrict__ in, const int32_t *__restrict__ vid_of, double *out,
                                  int n, int accumulate) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
@@ -1672,7 +1701,6 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t
   a.dis = d->dis;
   a.dis_sh = d->dis_sh;
   a.ch = d->ch;
-  a.anc = d->anc;
   a.lab_off = d->lab_off;
   a.depth = d->depth;
   a.send = d->send;
@@ -1685,12 +1713,16 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t
   a.out_rec = d->rec[buf];
   a.out_hop = d->hop[buf];
   a.maxhop = d->maxhop[buf];
-  a.aend = d->aend;
+  a.src_rows = d->src_rows[buf];
+  a.src_stride = d->hmax_pad;
   a.bits = d->packed_bits;
   a.err = d->err;
   a.wait_spins = row_wait_spins();
   const int groups = (ns + p.G - 1) / p.G;
   CK(cudaMemsetAsync(d->maxhop[buf], 0, (size_t)ns * 4, st));
+  k_src_rows<<<(ns + 127) / 128, 128, 0, st>>>(src, ns, d->depth, d->parent, d->send, d->hmax_pad, d->src_rows[buf]);
+  CK(cudaGetLastError());
+  d->launches++;
   std::pair<cudaEvent_t, cudaEvent_t> ev{};
   if (d->profiling) {
     ev = take_events(d->ev_lab, d->ev_lab_used);
@@ -1798,11 +1830,11 @@ void launch_vid_to_tid(DeviceState *d, const int32_t *vids, int32_t *tids, int32
 static void free_scratch(DeviceState *d) {
   sweep_cache_free(d);
   for (int b = 0; b < 2; b++) {
-    void *q[] = {d->rec[b], d->hop[b], d->order[b], d->lcnt[b], d->src[b], d->maxhop[b]};
+    void *q[] = {d->rec[b], d->hop[b], d->order[b], d->lcnt[b], d->src[b], d->maxhop[b], d->src_rows[b]};
     for (void *p : q)
       if (p) cudaFree(p);
     d->rec[b] = nullptr;
-    d->hop[b] = d->order[b] = d->lcnt[b] = d->src[b] = d->maxhop[b] = nullptr;
+    d->hop[b] = d->order[b] = d->lcnt[b] = d->src[b] = d->maxhop[b] = d->src_rows[b] = nullptr;
   }
   d->bytes -= d->scratch_bytes;
   d->scratch_bytes = 0;
@@ -1812,7 +1844,7 @@ static void free_scratch(DeviceState *d) {
 static void alloc_scratch(Handle &h, DeviceState *d) {
   const Index &ix = h.host;
   const int64_t before = d->bytes;
-  const size_t per_slot = (size_t)d->n_pad * (16 + 4 + 4) + (size_t)2 * (d->n_pad + 2) * 4 + 4;
+  const size_t per_slot = (size_t)d->n_pad * (16 + 4 + 4) + (size_t)2 * (d->n_pad + 2) * 4 + 4 + (size_t)8 * d->hmax_pad;
   size_t free_b = 0, total_b = 0;
   CK(cudaMemGetInfo(&free_b, &total_b));
   int32_t chunk = h.tuning.chunk;
@@ -1831,6 +1863,7 @@ static void alloc_scratch(Handle &h, DeviceState *d) {
     d->lcnt[b] = dmalloc<int32_t>(d, (size_t)chunk * 2 * (d->n_pad + 2));
     d->src[b] = dmalloc<int32_t>(d, (size_t)chunk);
     d->maxhop[b] = dmalloc<int32_t>(d, (size_t)chunk);
+    d->src_rows[b] = dmalloc<int32_t>(d, (size_t)chunk * 2 * d->hmax_pad);
   }
   d->scratch_bytes = d->bytes - before;
 }
@@ -1992,9 +2025,10 @@ __global__ void __launch_bounds__(256) k_fill_node_cta(FillArgs f, const int32_t
   }
 }
 
-__global__ void k_shift_left(const int32_t *__restrict__ in, int32_t *__restrict__ out, int64_t n, int bits) {
+// x[i] <<= bits in place (the packed-key scan's pre-shifted label distances)
+__global__ void k_shift_left(int32_t *x, int64_t n, int bits) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = (int32_t)((uint32_t)in[i] << bits);
+    x[i] = (int32_t)((uint32_t)x[i] << bits);
 }
 
 __global__ void k_max_i32(const int32_t *__restrict__ x, int64_t n, int32_t *out) {
@@ -2078,6 +2112,7 @@ static DeviceState *new_state(Handle &h, int device) {
   }
   d->vid_of = dupload(d, ix.vid_of, st);
   d->tid_of = dupload(d, ix.tid_of, st);
+  d->parent = dupload(d, ix.parent, st);
   d->lab_off = dupload(d, ix.lab_off, st);
   {
     double wsum = 0.0;
@@ -2098,11 +2133,11 @@ static void finish_state(Handle &h, DeviceState *d) {
     const uint64_t room = (uint64_t)1 << (32 - B);
     d->packed_bits = (ix.kind != IndexKind::CSR && B <= 16 && 2ull * (uint64_t)std::max(ix.max_label, 0) + 2 < room) ? B : 0;
   }
-  if (d->packed_bits) {  // label distances pre-shifted by B for the packed kernel (one add per entry)
+  if (d->packed_bits) {  // label distances pre-shifted by B, in place (one add per entry in the scan)
     const int64_t L = ix.lab_off[ix.n];
-    d->dis_sh = dmalloc<int32_t>(d, (size_t)L);
-    k_shift_left<<<148 * 8, 256, 0, st>>>(d->dis, d->dis_sh, L, d->packed_bits);
+    k_shift_left<<<148 * 8, 256, 0, st>>>(d->dis, L, d->packed_bits);
     CK(cudaGetLastError());
+    d->dis_sh = d->dis;
   }
   alloc_scratch(h, d);
   d->bc_tid = dmalloc<double>(d, ix.n);
@@ -2124,9 +2159,7 @@ void device_upload(Handle &h, int device) {
   try {
     d = new_state(h, device);
     cudaStream_t st = d->s_label;
-    d->dis = dupload(d, ix.dis, st);
-    d->anc = dupload(d, ix.anc, st);
-    d->aend = dupload(d, ix.aend, st);
+    d->dis = dupload(d, ix.dis, st);  // ancestor ids and subtree ends stay on the host
     if (ix.kind == IndexKind::MHL) {
       d->ch = dmalloc<int2>(d, ix.ch.size() / 2);
       CK(cudaMemcpyAsync(d->ch, ix.ch.data(), ix.ch.size() * 4, cudaMemcpyHostToDevice, st));
@@ -2146,11 +2179,8 @@ void device_build(Handle &h, int device, const Separators &seps) {
     cudaStream_t st = d->s_label;
     const int64_t L = ix.lab_off[ix.n];
     d->dis = dmalloc<int32_t>(d, (size_t)L);
-    d->anc = dmalloc<int32_t>(d, (size_t)L);
-    d->aend = dmalloc<int32_t>(d, (size_t)L);
     CK(cudaMemsetAsync(d->dis, 0, (size_t)L * 4, st));
-    CK(cudaMemsetAsync(d->anc, 0, (size_t)L * 4, st));
-    CK(cudaMemsetAsync(d->aend, 0, (size_t)L * 4, st));
+
     const bool mhl = ix.kind == IndexKind::MHL;
     if (mhl) {
       d->ch = dmalloc<int2>(d, (size_t)L);
@@ -2184,26 +2214,30 @@ void device_build(Handle &h, int device, const Separators &seps) {
       }
     }
     // temporaries of the fill, freed at the end
-    int32_t *d_nodes = nullptr, *d_parent = nullptr, *d_max = nullptr;
+    // per-entry ancestor ids and subtree ends (f_anc, f_aend): needed while rows are filled (a row
+    // reads its ancestors' entries), freed with the other temporaries once the fill is done
+    int32_t *d_nodes = nullptr, *d_max = nullptr, *f_anc = nullptr, *f_aend = nullptr;
     int64_t *d_soff = nullptr;
     int4 *d_sep = nullptr;
     auto free_tmp = [&] {
-      void *q[] = {d_nodes, d_parent, d_max, d_soff, d_sep};
+      void *q[] = {d_nodes, d_max, d_soff, d_sep, f_anc, f_aend};
       for (void *p : q)
         if (p) cudaFree(p);
     };
     try {
       CK(cudaMalloc(&d_nodes, nodes.size() * 4));
-      CK(cudaMalloc(&d_parent, ix.parent.size() * 4));
+      CK(cudaMalloc(&f_anc, (size_t)std::max<int64_t>(L, 1) * 4));
+      CK(cudaMalloc(&f_aend, (size_t)std::max<int64_t>(L, 1) * 4));
+      CK(cudaMemsetAsync(f_anc, 0, (size_t)L * 4, st));
+      CK(cudaMemsetAsync(f_aend, 0, (size_t)L * 4, st));
       CK(cudaMalloc(&d_soff, seps.off.size() * 8));
       CK(cudaMalloc(&d_sep, std::max<size_t>(16, seps.ent.size() * 4)));
       CK(cudaMalloc(&d_max, 4));
       CK(cudaMemcpyAsync(d_nodes, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice, st));
-      CK(cudaMemcpyAsync(d_parent, ix.parent.data(), ix.parent.size() * 4, cudaMemcpyHostToDevice, st));
       CK(cudaMemcpyAsync(d_soff, seps.off.data(), seps.off.size() * 8, cudaMemcpyHostToDevice, st));
       if (!seps.ent.empty()) CK(cudaMemcpyAsync(d_sep, seps.ent.data(), seps.ent.size() * 4, cudaMemcpyHostToDevice, st));
       CK(cudaMemsetAsync(d_max, 0, 4, st));
-      FillArgs f{d->depth, d_parent, d->send, d->lab_off, d_soff, d_sep, d->dis, d->ch, d->anc, d->aend};
+      FillArgs f{d->depth, d->parent, d->send, d->lab_off, d_soff, d_sep, d->dis, d->ch, f_anc, f_aend};
       const size_t max_stage = (size_t)stage_cap * kFillStageBytes;
       CK(cudaFuncSetAttribute(k_fill_node_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_stage));
       CK(cudaFuncSetAttribute(k_fill_node_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_stage));
@@ -2253,11 +2287,10 @@ void device_download_rows(Handle &h) {
   CK(cudaSetDevice(d->device));
   const size_t L = (size_t)ix.lab_off[ix.n];
   ix.dis.resize(L);
-  ix.anc.resize(L);
-  ix.aend.resize(L);
   CK(cudaMemcpy(ix.dis.data(), d->dis, L * 4, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(ix.anc.data(), d->anc, L * 4, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(ix.aend.data(), d->aend, L * 4, cudaMemcpyDeviceToHost));
+  if (d->packed_bits)  // the device keeps them shifted for the packed-key scan
+    for (int32_t &x : ix.dis) x = (int32_t)((uint32_t)x >> d->packed_bits);
+  fill_ancestor_rows(ix);  // not kept on the device: rebuilt from the parent links
   if (ix.kind == IndexKind::MHL) {
     ix.ch.resize(2 * L);
     CK(cudaMemcpy(ix.ch.data(), d->ch, L * 8, cudaMemcpyDeviceToHost));
@@ -2270,8 +2303,8 @@ void device_release(Handle &h) {
   if (!d) return;
   cudaSetDevice(d->device);
   cudaDeviceSynchronize();
-  void *ptrs[] = {d->depth, d->send, d->arc_off, d->arc_head, d->arc_w, d->arc_rng, d->arc_hw, d->arc4, d->vid_of, d->tid_of, d->lab_off, d->dis,
-                  d->dis_sh, d->anc, d->aend, d->ch, d->bc_tid, d->bc_vid, d->err, d->grid_ctl, d->sources};
+  void *ptrs[] = {d->depth, d->send, d->arc_off, d->arc_head, d->arc_w, d->arc_rng, d->arc_hw, d->arc4, d->vid_of, d->tid_of, d->parent,
+                  d->lab_off, d->dis, d->ch, d->bc_tid, d->bc_vid, d->err, d->grid_ctl, d->sources};  // dis_sh aliases dis
   for (void *p : ptrs)
     if (p) cudaFree(p);
   free_scratch(d);
@@ -2482,7 +2515,9 @@ constexpr size_t kStaticOrder = kStaticHop + (size_t)kStaticMaxVertices * 4;    
 constexpr size_t kStaticLcnt = kStaticOrder + (size_t)kStaticMaxVertices * 4;       // int32[2*(max+2)]
 constexpr size_t kStaticBc = kStaticLcnt + (((size_t)2 * (kStaticMaxVertices + 2) * 4 + 255) / 256) * 256;  // double[max]
 constexpr size_t kStaticSrc = kStaticBc + (size_t)kStaticMaxVertices * 8;           // int32[64]
-constexpr size_t kStaticScratchBytes = kStaticSrc + 256;
+constexpr int32_t kStaticMaxHeight = 8192;  // source-row capacity (the label kernel's own limit is lower)
+constexpr size_t kStaticSrcRows = kStaticSrc + 256;                                  // int32[2*height]
+constexpr size_t kStaticScratchBytes = kStaticSrcRows + (size_t)2 * kStaticMaxHeight * 4;
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
@@ -2519,7 +2554,7 @@ void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *s
     // the one-source label kernel keeps a source row and one row per warp in shared memory
     // (44 B per tree level): taller trees need the batched path or a CSR index
     const size_t budget = (size_t)std::max(48 * 1024, d->smem_optin) - 2048;
-    if ((size_t)44 * d->hmax_pad > budget)
+    if ((size_t)44 * d->hmax_pad > budget || d->hmax_pad > kStaticMaxHeight)
       throw Error(QBC_EINVAL, "tree height " + std::to_string(h.host.tree_height) + " exceeds the " +
                                   std::to_string(budget / 44) + " levels the static-scratch entry point's label kernel holds in "
                                   "shared memory; use qbc_bc_sources_device or a QBC_INDEX_CSR index");
@@ -2542,9 +2577,14 @@ void host_bc_source_static(Handle &h, int32_t source0, double *d_bc_vid, void *s
   } else {
     const LabelPlan p = plan_label(h, d, 1, true);
     LabelArgs la{};
+    int32_t *src_rows = reinterpret_cast<int32_t *>(base + kStaticSrcRows);
+    k_src_rows<<<1, 32, 0, st>>>(src, 1, d->depth, d->parent, d->send, d->hmax_pad, src_rows);
+    CK(cudaGetLastError());
     la.dis = d->dis;
     la.ch = d->ch;
-    la.anc = d->anc;
+    la.src_rows = src_rows;
+    la.src_stride = d->hmax_pad;
+    la.bits = d->packed_bits;
     la.lab_off = d->lab_off;
     la.depth = d->depth;
     la.send = d->send;

@@ -67,10 +67,14 @@ struct DeviceState {
   int32_t *depth = nullptr, *send = nullptr, *arc_off = nullptr, *arc_head = nullptr, *arc_w = nullptr;
   int2 *arc_rng = nullptr, *arc_hw = nullptr;
   int4 *arc4 = nullptr;  // per vertex 2 x int4: (head, weight) of its first four arcs (see k_dependency_cta_pipe)
-  int32_t *vid_of = nullptr, *tid_of = nullptr, *dis = nullptr, *anc = nullptr, *aend = nullptr;
+  int32_t *vid_of = nullptr, *tid_of = nullptr, *parent = nullptr;
+  // label distances: one array, shifted left in place by packed_bits when the packed-key scan
+  // applies (dis_sh then aliases it); no per-entry ancestor ids or subtree ends are kept -- each
+  // launch derives its sources' rows from the parent links (k_src_rows)
+  int32_t *dis = nullptr;
   int32_t packed_bits = 0;  // > 0: the packed-key label scan applies
   int32_t sweep_delta_auto = 1;  // CSR sweep's default bucket width (twice the mean arc weight)
-  int32_t *dis_sh = nullptr;  // dis << packed_bits (packed kernel only)
+  int32_t *dis_sh = nullptr;  // = dis when packed_bits > 0 (the packed kernel's name for it)
   int64_t *lab_off = nullptr;
   int2 *ch = nullptr;
   // scratch: one buffer of `chunk` source slots (index 1 unused)
@@ -81,6 +85,7 @@ struct DeviceState {
   int32_t *lcnt[2] = {nullptr, nullptr};
   int32_t *src[2] = {nullptr, nullptr};
   int32_t *maxhop[2] = {nullptr, nullptr};
+  int32_t *src_rows[2] = {nullptr, nullptr};  // per slot: source's ancestors, then their subtree ends (hmax_pad each)
   double *bc_tid = nullptr;
   double *bc_vid = nullptr;
   int32_t *sources = nullptr;  // staging for host source lists

@@ -454,24 +454,7 @@ void make_tree(const Graph &g, const Elimination &el, Index &ix, bool host_rows 
     ix.depth_sum += ix.depth[t];
   }
   ix.lab_off[n] = o;
-  if (host_rows) {
-  // ancestor rows: a row is its parent's row plus the node itself (preorder: parent first)
-  ix.anc.assign((size_t)o, 0);
-  for (int32_t t = 0; t < n; t++) {
-    const int32_t h = ix.depth[t];
-    int32_t *row = ix.anc.data() + ix.lab_off[t];
-    if (t > 0) {
-      const int32_t *prow = ix.anc.data() + ix.lab_off[ix.parent[t]];
-      std::copy(prow, prow + (h - 1), row);
-    }
-    row[h - 1] = t;
-  }
-  ix.aend.assign((size_t)o, 0);
-  for (int32_t t = 0; t < n; t++) {
-    const int64_t b = ix.lab_off[t];
-    for (int32_t j = 0; j < ix.depth[t]; j++) ix.aend[b + j] = ix.send[ix.anc[b + j]];
-  }
-  }
+  if (host_rows) fill_ancestor_rows(ix);
   // arcs in tid space
   ix.arc_off.assign((size_t)n + 1, 0);
   ix.arc_head.resize(g.head.size());
@@ -505,6 +488,28 @@ void fill_rows(const Index &ix, int nthreads, F &&f) {
   });
 }
 }  // namespace
+
+void fill_ancestor_rows(Index &ix) {
+  const int32_t n = ix.n;
+  const int64_t o = ix.lab_off.empty() ? 0 : ix.lab_off[n];
+  // a row is its parent's row plus the node itself (preorder: parent first)
+  ix.anc.assign((size_t)o, 0);
+  for (int32_t t = 0; t < n; t++) {
+    const int32_t h = ix.depth[t];
+    if (h <= 0) continue;
+    int32_t *row = ix.anc.data() + ix.lab_off[t];
+    if (ix.parent[t] >= 0) {
+      const int32_t *prow = ix.anc.data() + ix.lab_off[ix.parent[t]];
+      std::copy(prow, prow + (h - 1), row);
+    }
+    row[h - 1] = t;
+  }
+  ix.aend.assign((size_t)o, 0);
+  for (int32_t t = 0; t < n; t++) {
+    const int64_t b = ix.lab_off[t];
+    for (int32_t j = 0; j < ix.depth[t]; j++) ix.aend[b + j] = ix.send[ix.anc[b + j]];
+  }
+}
 
 // Elimination (min-degree for MHL, the order file's for H2H) and tree, without label rows; the
 // separator list of each tree node goes to `seps` in tid space for the device row fill.

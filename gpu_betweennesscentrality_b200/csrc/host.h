@@ -71,6 +71,9 @@ struct Separators {
 // Elimination and tree only (no label rows: dis/ch/anc/aend stay empty); max_label is unknown (0).
 Index prepare_index(const Graph &g, IndexKind kind, const std::vector<int32_t> *node_order, Separators &seps);
 
+// Per-entry ancestor ids (anc) and their subtree ends (aend) of every row, from the tree links
+// (a row is its parent's row plus the node itself).
+void fill_ancestor_rows(Index &ix);
 // TreeCount-equivalent index (distance + count + max hop) by min-degree elimination.
 Index build_mhl(const Graph &g, int nthreads);
 // H2H distance index from an order file (node_order[vid] = contraction rank).
