@@ -273,15 +273,17 @@ def plain_rate(idx, sources, k):
 
 # ------------------------------------------------------------------------------- rooflines
 def label_roofline(idx, shard, n, stats, steps, peak, peak_src, sm_mhz):
-    """Dominant kernel of the 50k step: the packed label scan.  DRAM model per launch: target rows
-    copied once per 32-source CTA group, each up to the group's deepest LCA depth (4 B per entry,
-    exact from the index), plus the (dist, count, rho) records and hop layers written (20 B per
-    pair); cross-checked against ncu in profiles/k_label_scan_packed_50k.md (model 9.12 GB, ncu
-    9.80 GB per 4,096-source launch).  The algorithmic figure of the workload's byte model (12 B
+    """Dominant kernel of the label path: the packed label scan.  DRAM model per launch: target rows
+    copied once per CTA group of sources (32; 16 for the tall-tree form), each up to the group's
+    deepest LCA depth (4 B per entry, exact from the index), plus the (dist, count, rho) records
+    and hop layers written (20 B per pair); cross-checked against ncu in
+    profiles/k_label_scan_packed_50k.md (model 9.12 GB, ncu 9.80 GB per 4,096-source launch).  The algorithmic figure of the workload's byte model (12 B
     per label entry scanned + 12 B per pair) is given as effective_bw: rows are reused by 32
     sources, so it exceeds the HBM peak."""
     ns = len(shard)
-    group = idx.group_entries(shard, 32)
+    per_cta = idx.label_group() or 32
+    tall = per_cta == 16
+    group = idx.group_entries(shard, per_cta)
     scan = idx.scan_entries(shard)
     label_ms_step = stats["label_ms"] / steps
     launches_step = max(1.0, stats["label_launches"] / steps)
@@ -291,19 +293,22 @@ def label_roofline(idx, shard, n, stats, steps, peak, peak_src, sm_mhz):
     achieved = dram_step / launches_step / (launch_ms / 1e3) / 1e9
     effective = algo_step / launches_step / (launch_ms / 1e3) / 1e9
     ent_per_clk = scan / (label_ms_step / 1e3) / (sm_mhz * 1e6) / 148.0
+    smem_roof = 256.0 / 6.0 if tall else 25.6
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": None, "peak_source": peak_src, "kernel": "k_label_scan_packed",
+            "traffic": None, "peak_source": peak_src,
+            "kernel": "k_label_scan_tall" if tall else "k_label_scan_packed", "sources_per_cta": per_cta,
             "dram_model_bytes_per_launch": dram_step / launches_step, "launch_ms": launch_ms,
             "launches_per_step": launches_step, "label_ms_per_step": label_ms_step,
             "dependency_ms_per_step": stats["dep_ms"] / steps,
             "effective_bw": {"achieved": effective, "unit": "GB/s", "frac_of_hbm_peak": effective / peak,
                              "algorithmic_bytes_per_launch": algo_step / launches_step},
-            "compute_roof": {"unit": "label entries/clk/SM", "achieved": ent_per_clk, "peak": 25.6,
-                             "frac": ent_per_clk / 25.6, "issue_peak": 128.0 / 3.5,
-                             "note": "the roof the kernel runs against: 5 shared-memory wavefronts per 128 "
-                                     "lane-entries (25.6) and 3.5 instructions per pair-entry at 128 lane-"
-                                     "instructions/clk/SM (issue_peak); kernels moving 40-60 % fewer wavefronts "
-                                     "measured no faster, so issue and latency bind"},
+            "compute_roof": {"unit": "label entries/clk/SM", "achieved": ent_per_clk, "peak": smem_roof,
+                             "frac": ent_per_clk / smem_roof, "issue_peak": 128.0 / 3.5,
+                             "note": ("tall-tree form: 6 shared-memory wavefronts per 256 lane-entries (two "
+                                      "targets per warp, 16 source rows per load: 42.7)" if tall else
+                                      "5 shared-memory wavefronts per 128 lane-entries (25.6)") +
+                                     " and 3.5 instructions per pair-entry at 128 lane-instructions/clk/SM "
+                                     "(issue_peak)"},
             "note": "frac = modelled DRAM bytes per launch / launch time / measured HBM copy bandwidth; traffic "
                     "is not measured in this run (ncu figures for the same kernel are in profiles/)"}
 

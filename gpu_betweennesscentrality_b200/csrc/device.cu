@@ -574,6 +574,246 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
   if (COUNTS && fin && have && a.maxhop) atomicMax(a.maxhop + first + lane, mh);
 }
 
+// ------------------------------------------------------------------------------- K1 + K2, tall trees
+// Packed-key label scan for trees too tall for the 32-source CTA to hold its source rows in shared
+// memory (MHLQBC.cu:379-392 is the scan it replaces).  A CTA takes 16 sources, so whole rows fit
+// (16 x height x 4 bytes: 175 KB at height 2,728).  Each warp scans two targets at once: lanes
+// 0-15 pair the 16 sources with target A, lanes 16-31 with target B, so one 16-byte shared load of
+// the source keys serves both halves (16 distinct rows: 2 wavefronts instead of 4 for 32 rows) and
+// each half's target row is a broadcast.  Target rows stream through a per-half ring of R blocks of
+// 64 entries filled by cp.async (16 bytes per lane, R - 1 blocks ahead of the scan, only up to the
+// half's deepest LCA), so no entry of a scan is read from global memory.  Keys, tie detection,
+// count/hop gathers and the chunk-blocked output are those of k_label_scan_packed.
+constexpr int kTallSources = 16;
+constexpr int kTallRing = 4;                                   // blocks per half-warp ring
+constexpr int kTallBlock = 64;                                 // entries per block (16 lanes x 4)
+constexpr int kTallHalfWords = kTallRing * kTallBlock + 4;     // +4: the halves start in different bank groups
+constexpr int kTallRingWords = 2 * kTallHalfWords;            // per warp
+constexpr int kTallStageWords = kTallSources * 10 * 2 + kTallSources * 12;  // (dist, count) x 10 + hops x 12 per slot
+
+__host__ __device__ constexpr size_t tall_smem(int warps, int S) {
+  return (size_t)kTallSources * S * 4 + (size_t)warps * (kTallRingWords + kTallStageWords) * 4;
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool in) {
+  // src-size 0: nothing is read and the 16 bytes are zero-filled
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(in ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <bool COUNTS, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) {
+  constexpr int G = kTallSources;
+  extern __shared__ int4 smem4[];
+  uint32_t *s_key = reinterpret_cast<uint32_t *>(smem4);
+  const int S = a.stride;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int half = lane >> 4, sl = lane & 15;
+  uint32_t *ring = s_key + G * S + warp * kTallRingWords + half * kTallHalfWords;
+  int32_t *stage = reinterpret_cast<int32_t *>(s_key + G * S + nwarps * kTallRingWords) + warp * kTallStageWords;
+  int2 *sdc = reinterpret_cast<int2 *>(stage);          // slot x 10: (dist, count) of 8 targets
+  int2 *sdc2 = sdc + sl * 10;
+  int32_t *shp = stage + G * 10 * 2;                    // slot x 12: hop layers of 8 targets
+  int32_t *shp1 = shp + sl * 12;
+  __shared__ int32_t s_h[G];
+  __shared__ int64_t s_off[G];
+  const int first = blockIdx.y * G;
+  if (first >= a.ns) return;
+  const int gcount = min(G, a.ns - first);
+  const uint32_t B = (uint32_t)a.bits, mask = (1u << B) - 1u;
+  if (threadIdx.x < G) {
+    const int i = threadIdx.x;
+    const int s = i < gcount ? a.src[first + i] : 0;
+    s_h[i] = i < gcount ? a.depth[s] : 0;
+    s_off[i] = a.lab_off[s];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < G * S; idx += blockDim.x) {
+    const int i = idx / S, j = idx - i * S;
+    uint32_t key = 0xffffffffu;
+    if (i < gcount && j < s_h[i]) key = (uint32_t)a.dis_sh[s_off[i] + j] | (uint32_t)j;
+    s_key[idx] = key;
+  }
+  __syncthreads();
+
+  const bool have = sl < gcount;
+  const int hs = have ? s_h[sl] : 1;
+  const int64_t soff = s_off[sl];
+  const uint32_t *srow = s_key + sl * S;
+  const int32_t *lo = a.src_rows + (size_t)(first + (have ? sl : 0)) * 2 * a.src_stride;
+  const int32_t *hi = lo + a.src_stride;
+  const int nsteps = 32 - __clz(hs);
+  int mh = 0;
+
+  const int nchunk = a.n_pad >> 3;
+  const int cbeg = (int)((int64_t)nchunk * blockIdx.x / a.split);
+  const int cend = (int)((int64_t)nchunk * (blockIdx.x + 1) / a.split);
+  for (int c = cbeg + warp; c < cend; c += nwarps) {
+    const int t0 = c << 3;
+    const int kend = min(8, a.n - t0);
+    const int tb = t0 + 4 * half;  // this half's targets: tb .. tb + 3
+    // deepest ancestor interval of this lane's source holding tb (binary search)
+    int J = 0;
+    if (tb < a.n) {
+      int h = have ? hs : 1;
+      for (int it = 0; it < nsteps; it++) {
+        if (h - J > 1) {
+          const int mid = (J + h) >> 1;
+          const bool p = (__ldg(lo + mid) <= tb) && (tb < __ldg(hi + mid));
+          J = p ? mid : J;
+          h = p ? h : mid;
+        }
+      }
+    }
+    int hiJ = have ? __ldg(hi + J) : 0x7fffffff;
+    int loN = (have && J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
+    uint32_t pending = 0;
+    for (int k = 0; k < 4; k++) {
+      const int t = tb + k;
+      const bool tv = 4 * half + k < kend;
+      if (have && tv && k > 0) {  // advance the interval (targets grow by one)
+        if (t >= hiJ) {
+          do { J--; hiJ = __ldg(hi + J); } while (t >= hiJ);
+          loN = __ldg(lo + J + 1);
+        } else if (t == loN) {
+          J++;
+          hiJ = __ldg(hi + J);
+          loN = (J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
+        }
+      }
+      const int hl = (have && tv) ? J + 1 : 0;
+      int hh = hl;  // the half's deepest scan, then the warp's
+#pragma unroll
+      for (int o = 8; o >= 1; o >>= 1) hh = max(hh, __shfl_xor_sync(kFull, hh, o));
+      const int lim = (hh + 3) & ~3;  // entries of this half's target row to bring in
+      const int nb = (max(hh, __shfl_xor_sync(kFull, hh, 16)) + kTallBlock - 1) / kTallBlock;
+      const int64_t toff = tv ? a.lab_off[t] : 0;
+      const int32_t *trow = a.dis_sh + toff;
+      auto issue = [&](int b) {  // block b of this half's row; an empty group past the last block
+        if (b < nb) {
+          const int e = b * kTallBlock + 4 * sl;
+          cp_async16(ring + (b % kTallRing) * kTallBlock + 4 * sl, e < lim ? trow + e : trow, e < lim);
+        }
+        cp_async_commit();
+      };
+      __syncwarp();  // the ring's slots are no longer read for the previous target
+#pragma unroll
+      for (int b = 0; b < kTallRing - 1; b++) issue(b);
+      uint32_t m1 = 0xffffffffu, m2 = 0xffffffffu, n1 = 0xffffffffu, n2 = 0xffffffffu;
+      for (int b = 0; b < nb; b++) {
+        __syncwarp();  // block b - 1's slot is free
+        issue(b + kTallRing - 1);
+        cp_async_wait<kTallRing - 1>();  // this lane's part of block b has landed
+        __syncwarp();                     // and every lane's
+        const uint32_t *tbuf = ring + (b % kTallRing) * kTallBlock;
+        const uint32_t *xs = srow + b * kTallBlock;
+        const int hm = min(hl - b * kTallBlock, kTallBlock);
+        const int full8 = hm > 0 ? (hm & ~7) : 0;
+        int j = 0;
+        for (; j < full8; j += 8) {
+          const uint4 x = *reinterpret_cast<const uint4 *>(xs + j);
+          const uint4 y = *reinterpret_cast<const uint4 *>(tbuf + j);
+          const uint4 x2 = *reinterpret_cast<const uint4 *>(xs + j + 4);
+          const uint4 y2 = *reinterpret_cast<const uint4 *>(tbuf + j + 4);
+          const uint32_t v0 = x.x + y.x, v1 = x.y + y.y, v2 = x.z + y.z, v3 = x.w + y.w;
+          const uint32_t u0 = x2.x + y2.x, u1 = x2.y + y2.y, u2 = x2.z + y2.z, u3 = x2.w + y2.w;
+          m1 = __vimin3_u32(m1, v0, v1);
+          n1 = __vimin3_u32(n1, u0, u1);
+          m1 = __vimin3_u32(m1, v2, v3);
+          n1 = __vimin3_u32(n1, u2, u3);
+          m2 = __vimin3_u32(m2, v0 ^ mask, v1 ^ mask);
+          n2 = __vimin3_u32(n2, u0 ^ mask, u1 ^ mask);
+          m2 = __vimin3_u32(m2, v2 ^ mask, v3 ^ mask);
+          n2 = __vimin3_u32(n2, u2 ^ mask, u3 ^ mask);
+        }
+        for (; j < hm; j += 4) {
+          const uint4 x = *reinterpret_cast<const uint4 *>(xs + j);
+          const uint4 y = *reinterpret_cast<const uint4 *>(tbuf + j);
+          const uint32_t v0 = x.x + y.x;
+          const uint32_t v1 = (j + 1 < hm) ? x.y + y.y : 0xffffffffu;
+          const uint32_t v2 = (j + 2 < hm) ? x.z + y.z : 0xffffffffu;
+          const uint32_t v3 = (j + 3 < hm) ? x.w + y.w : 0xffffffffu;
+          m1 = __vimin3_u32(m1, v0, v1);
+          m1 = __vimin3_u32(m1, v2, v3);
+          m2 = __vimin3_u32(m2, v0 ^ mask, (j + 1 < hm) ? v1 ^ mask : 0xffffffffu);
+          m2 = __vimin3_u32(m2, (j + 2 < hm) ? v2 ^ mask : 0xffffffffu, (j + 3 < hm) ? v3 ^ mask : 0xffffffffu);
+        }
+      }
+      m1 = min(m1, n1);
+      m2 = min(m2, n2);
+      const uint32_t dist = m1 >> B;
+      int cnt = 0, hop = 0;
+      if (COUNTS && have && tv) {
+        if ((m1 ^ m2) == mask) {
+          cnt = (int)(m1 & mask);  // the minimising entry; counts resolved after the chunk
+          pending |= 1u << k;
+        } else {  // a tie: sum over every minimising entry (target row from global memory)
+          unsigned cc = 0;
+          int hx = 0;
+          for (int q = 0; q < hl; q++) {
+            const uint32_t dq = (srow[q] + (uint32_t)__ldg(trow + q)) >> B;
+            if (dq == dist) {
+              const int2 cs = __ldg(a.ch + soff + q), ct = __ldg(a.ch + toff + q);
+              cc += (unsigned)cs.x * (unsigned)ct.x;
+              hx = max(hx, cs.y + ct.y);
+            }
+          }
+          cnt = (int)cc;
+          hop = hx;
+        }
+      }
+      if (have && tv) {
+        sdc2[4 * half + k] = make_int2((int)dist, cnt);
+        if (COUNTS) shp1[4 * half + k] = hop;
+      } else if (have) {
+        sdc2[4 * half + k] = make_int2(0, 0);
+        if (COUNTS) shp1[4 * half + k] = 0;
+      }
+    }
+    if (COUNTS && have && pending) {
+      int2 cs4[4], ct4[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (pending & (1u << k)) {
+          const int jm = sdc2[4 * half + k].y;
+          cs4[k] = __ldg(a.ch + soff + jm);
+          ct4[k] = __ldg(a.ch + a.lab_off[tb + k] + jm);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (pending & (1u << k)) {
+          sdc2[4 * half + k].y = (int)((unsigned)cs4[k].x * (unsigned)ct4[k].x);
+          shp1[4 * half + k] = cs4[k].y + ct4[k].y;
+        }
+      }
+    }
+    if (COUNTS && have) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) mh = max(mh, shp1[4 * half + k]);
+    }
+    __syncwarp();
+    {  // the warp's 16 slots x 8 targets are one contiguous block of records
+      int4 *grec = a.out_rec + blk(first, t0, a.ns);
+      for (int p = lane; p < gcount * 8; p += 32) {
+        const int2 x = sdc[(p >> 3) * 10 + (p & 7)];
+        grec[p] = make_int4(x.x, x.y, 0, 0);
+      }
+      if (COUNTS) {
+        int4 *ghp = reinterpret_cast<int4 *>(a.out_hop + blk(first, t0, a.ns));
+        const int4 *shp4 = reinterpret_cast<const int4 *>(shp);
+        for (int p = lane; p < gcount * 2; p += 32) ghp[p] = shp4[(p >> 1) * 3 + (p & 1)];
+      }
+    }
+    __syncwarp();
+  }
+  cp_async_wait<0>();
+  if (COUNTS && have && a.maxhop) atomicMax(a.maxhop + first + sl, mh);
+}
+
 // ------------------------------------------------------------------------------- K1 + K2, target pairs
 // Variant of k_label_scan_packed that scans two targets per step: each lane's source-row words
 // are loaded from shared memory once and combined with both target rows, so a step moves 3 instead of
@@ -1654,8 +1894,49 @@ static void launch_label_pair(const Handle &h, const DeviceState *d, LabelArgs a
   CK(cudaGetLastError());
 }
 
+// Tall trees: the 16-source kernel when the 32-source one cannot hold whole rows (its scans would
+// read entries beyond the tile from global memory) and the label warps, tile and passes are not
+// tuned; the most warps (16, 12 or 8) whose shared memory holds the whole height.  0: not used.
+static int tall_stride(const DeviceState *d) {
+  int S = d->hmax_pad;
+  if (((S / 4) & 1) == 0) S += 4;  // odd in 16-byte units: rows 0-7 start in distinct bank groups
+  return S;
+}
+static int tall_warps(const Handle &h, const DeviceState *d) {
+  const Tuning &t = h.tuning;
+  if (t.label_sources == 32) return 0;
+  if (t.label_sources == 0 &&
+      (t.label_warps != 0 || t.label_tile > 0 || t.label_passes != 0 || packed_stride(h, d, 8) >= d->hmax_pad))
+    return 0;
+  const size_t budget = (size_t)std::max(0, d->smem_optin - 2048);
+  const int w = t.label_warps;
+  if ((w == 8 || w == 12 || w == 16) && tall_smem(w, tall_stride(d)) <= budget) return w;
+  for (int x : {16, 12, 8})
+    if (tall_smem(x, tall_stride(d)) <= budget) return x;
+  return 0;
+}
+
+template <bool C, int W>
+static void launch_label_tall(const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
+  const int S = tall_stride(d);
+  const size_t smem = tall_smem(W, S);
+  const int groups = (ns + kTallSources - 1) / kTallSources;
+  int split = std::max(1, (148 * 4 + groups - 1) / groups);
+  split = std::min(split, std::max(1, (d->n_pad / 8) / W));
+  a.stride = S;
+  a.split = split;
+  CK(cudaFuncSetAttribute(k_label_scan_tall<C, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(split, groups);
+  k_label_scan_tall<C, W><<<grid, W * 32, smem, st>>>(a);
+  CK(cudaGetLastError());
+}
+
 template <bool C>
 static void launch_label_packed(const Handle &h, const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
+  const int tw = tall_warps(h, d);
+  if (tw == 16) return launch_label_tall<C, 16>(d, a, ns, st);
+  if (tw == 12) return launch_label_tall<C, 12>(d, a, ns, st);
+  if (tw == 8) return launch_label_tall<C, 8>(d, a, ns, st);
   const int w = packed_warps(h, d);
   if (w == 12) launch_label_pair<C>(h, d, a, ns, st);
   else if (w == 16) launch_label_packed_w<C, 16>(h, d, a, ns, st);
@@ -1849,7 +2130,9 @@ static void alloc_scratch(Handle &h, DeviceState *d) {
   CK(cudaMemGetInfo(&free_b, &total_b));
   int32_t chunk = h.tuning.chunk;
   if (chunk <= 0) {
-    const size_t budget = std::min<size_t>(free_b / 4, (size_t)24 << 30);
+    // at most 20 GB: at 1M vertices (32 MB per slot) 608 slots, within 2-4 % of the throughput of
+    // 736-1,024 slots (24-33 GB), with the 12 B per entry index the whole state stays near 44 GB
+    const size_t budget = std::min<size_t>(free_b / 4, (size_t)20 << 30);
     chunk = (int32_t)std::max<size_t>(32, std::min<size_t>(4096, budget / per_slot));
     chunk = std::max(32, (chunk / 32) * 32);
   }
@@ -2402,6 +2685,13 @@ void device_stats(Handle &h, double *out) {
   out[2] = d->dep_ms;
   out[3] = (double)d->dep_launches;
   out[4] = (double)d->launches;
+}
+
+int32_t device_label_group(Handle &h) {
+  DeviceState *d = need_dev(h);
+  if (h.host.kind == IndexKind::CSR) return 0;
+  if (use_packed(h, d, false)) return tall_warps(h, d) ? kTallSources : 32;
+  return plan_label(h, d, std::max(1, d->chunk), false).G;
 }
 
 static int32_t *stage_sources(DeviceState *d, const int32_t *sources0, int32_t ns, int32_t n) {

@@ -22,6 +22,8 @@ struct Tuning {
   int32_t label_passes = 0;      // rows longer than the tile: 0/1 one pass + global tail, 2 several tile passes
   int32_t sweep_delta = 0;       // CSR index: distance bucket width of the shortest-path sweep; 0 = auto
   int32_t sweep_threads = 0;     // CSR index: threads per CTA of the sweep (256, 512 or 1024; 0 = 512)
+  int32_t label_sources = 0;     // packed-key label kernel: sources per CTA (32, or 16 with whole rows of
+                                 // tall trees in shared memory); 0 = auto
 };
 
 struct DeviceState;  // opaque, defined in device_state.h
@@ -57,6 +59,8 @@ void device_profiling(Handle &h, bool on);
 // out[0]=label ms, [1]=label launches, [2]=dependency ms, [3]=dependency launches, [4]=all launches
 // since the last device_profiling call; synchronises the device.
 void device_stats(Handle &h, double *out);
+// sources per CTA of the batched label scan under the current tuning (0: label-free index)
+int32_t device_label_group(Handle &h);
 // rows of each listed source in vid order (cnt/hop may be null)
 void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, uint32_t *cnt, int32_t *hop);
 

@@ -80,6 +80,51 @@ def test_packed_kernel_tiles_and_warps(g2k, warps, tile, passes):
     assert rel_err(bc, tc.bc(arcs, srcs)) <= BC_RTOL
 
 
+@pytest.mark.parametrize("warps", [0, 8, 12, 16])
+def test_tall_tree_kernel_forced_2k(g2k, warps):
+    """the tall-tree form of the packed scan (16 sources per CTA, two targets per warp, target rows
+    through a cp.async ring) forced on the 2k graph: a ragged last group of sources, target chunks
+    cut by n, ties -- rows bit-identical to the 32-source kernel's, BC against the oracle"""
+    n, u, v, w, g, idx, tc, arcs = g2k
+    srcs = np.arange(3, n, 11, dtype=np.int32)  # 182 sources: 11 groups of 16 and one of 6
+    idx.set_tuning(label_sources=32)
+    try:
+        assert idx.label_group() == 32
+        base = idx.rows(srcs)
+        idx.set_tuning(label_sources=16, label_warps=warps)
+        assert idx.label_group() == 16
+        alt = idx.rows(srcs)
+        bc = idx.bc_sources(srcs)
+    finally:
+        idx.set_tuning()
+    for a, b in zip(base, alt):
+        assert np.array_equal(a, b)
+    assert rel_err(bc, tc.bc(arcs, srcs)) <= BC_RTOL
+
+
+def test_tall_tree_kernel_unit_weight_ties():
+    """unit weights on a 40 x 40 lattice: most pairs have many shortest paths through several hubs
+    (the scan's tie branch); the tall-tree kernel's rows equal the oracle's"""
+    side = 40
+    edges = [(r * side + c, r * side + c + 1, 1) for r in range(side) for c in range(side - 1)]
+    edges += [(r * side + c, (r + 1) * side + c, 1) for r in range(side - 1) for c in range(side)]
+    nn, u, v, w = lines_of(edges, side * side)
+    g = _graph(nn, u, v, w)
+    idx = g.build_index()
+    tc = O.TreeCount(nn, u, v, w)
+    srcs = np.arange(0, nn, 37, dtype=np.int32)
+    idx.set_tuning(label_sources=16)
+    try:
+        d, c, h = idx.rows(srcs)
+        bc = idx.bc_sources(srcs)
+    finally:
+        idx.set_tuning()
+    for k, s in enumerate(srcs):
+        d0, c0, h0 = tc.rows(int(s))
+        assert np.array_equal(d[k], d0) and np.array_equal(c[k], c0) and np.array_equal(h[k], h0)
+    assert rel_err(bc, tc.bc(O.Arcs(nn, u, v, w), srcs)) <= BC_RTOL
+
+
 def test_bc_all_2k_matches_oracle_and_reference(g2k):
     n, u, v, w, g, idx, tc, arcs = g2k
     bc = idx.bc_all()
@@ -255,9 +300,10 @@ def test_50k_sampled_rows_and_partial_bc(graph_cache):
 
 
 def test_200k_tall_tree_rows_and_partial_bc(graph_cache):
-    """the 200k grid's tree (height 1,088) is taller than the label kernel's shared tile: entries
-    beyond it come from global memory (default), from further tile passes, or with 16 warps from a
-    longer global tail -- rows bit-exact and partial BC against the oracle in every case"""
+    """the 200k grid's tree (height 1,088) is taller than the 32-source kernel's shared tile: the
+    default is the tall-tree form (16 sources per CTA, whole rows in shared memory); the 32-source
+    kernel reads entries beyond its tile from global memory, takes further tile passes, or with 16
+    warps a longer global tail -- rows bit-exact and partial BC against the oracle in every case"""
     path = synth.cached_graph(graph_cache, 200000, seed=1)
     n, u, v, w = synth.read_graph_lines(path)
     g = Q.Graph(device=0)
@@ -269,7 +315,9 @@ def test_200k_tall_tree_rows_and_partial_bc(graph_cache):
     srcs = np.sort(rng.choice(n, 16, replace=False)).astype(np.int32)
     want = [tc.rows(int(s)) for s in srcs[:4]]
     try:
-        for tune in ({}, {"label_warps": 16}, {"label_passes": 2}, {"label_warps": 12}):
+        assert idx.label_group() == 16
+        for tune in ({}, {"label_sources": 32}, {"label_warps": 16}, {"label_passes": 2}, {"label_warps": 12},
+                     {"label_sources": 16, "label_warps": 8}):
             idx.set_tuning(**tune)
             d, c, h = idx.rows(srcs[:4])
             for k in range(4):
