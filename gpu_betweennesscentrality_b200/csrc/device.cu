@@ -580,19 +580,21 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
 // (16 x height x 4 bytes: 175 KB at height 2,728).  Each warp scans two targets at once: lanes
 // 0-15 pair the 16 sources with target A, lanes 16-31 with target B, so one 16-byte shared load of
 // the source keys serves both halves (16 distinct rows: 2 wavefronts instead of 4 for 32 rows) and
-// each half's target row is a broadcast.  Target rows stream through a per-half ring of R blocks of
-// 64 entries filled by cp.async (16 bytes per lane, R - 1 blocks ahead of the scan, only up to the
-// half's deepest LCA), so no entry of a scan is read from global memory.  Keys, tie detection,
-// count/hop gathers and the chunk-blocked output are those of k_label_scan_packed.
+// each half's target row is a broadcast.  Target rows stream through a per-half ring of RING blocks
+// of 64 entries filled by cp.async (16 bytes per lane, RING - 1 blocks ahead of the scan, only up
+// to the half's deepest LCA), so no entry of a scan is read from global memory.  Keys, tie
+// detection, count/hop gathers and the chunk-blocked output are those of k_label_scan_packed.
+// (Measured: 16 warps with a 3-block ring beat 12 warps with 4 at 1M, 9.3 vs 8.7 entries/clk/SM;
+// one stream over a chunk's four targets, instead of a ring refilled per target, was slower:
+// its per-block bookkeeping cost more than the latency it hid.)
 constexpr int kTallSources = 16;
-constexpr int kTallRing = 4;                                   // blocks per half-warp ring
-constexpr int kTallBlock = 64;                                 // entries per block (16 lanes x 4)
-constexpr int kTallHalfWords = kTallRing * kTallBlock + 4;     // +4: the halves start in different bank groups
-constexpr int kTallRingWords = 2 * kTallHalfWords;            // per warp
-constexpr int kTallStageWords = kTallSources * 10 * 2 + kTallSources * 12;  // (dist, count) x 10 + hops x 12 per slot
+constexpr int kTallBlock = 64;  // entries per block (16 lanes x 4)
+__host__ __device__ constexpr int tall_half_words(int ring) { return ring * kTallBlock + 4; }  // +4: halves in different bank groups
+__host__ __device__ constexpr int tall_ring_words(int ring) { return 2 * tall_half_words(ring); }  // per warp
+constexpr int kTallStageWords = kTallSources * 8 * 2 + kTallSources * 8;  // per warp: (dist, count) and hop of 16 x 8 pairs
 
-__host__ __device__ constexpr size_t tall_smem(int warps, int S) {
-  return (size_t)kTallSources * S * 4 + (size_t)warps * (kTallRingWords + kTallStageWords) * 4;
+__host__ __device__ constexpr size_t tall_smem(int warps, int ring, int S) {
+  return (size_t)kTallSources * S * 4 + (size_t)warps * (tall_ring_words(ring) + kTallStageWords) * 4;
 }
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src, bool in) {
@@ -604,7 +606,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-template <bool COUNTS, int WARPS>
+template <bool COUNTS, int WARPS, int RING>
 __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) {
   constexpr int G = kTallSources;
   extern __shared__ int4 smem4[];
@@ -612,12 +614,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
   const int S = a.stride;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const int half = lane >> 4, sl = lane & 15;
-  uint32_t *ring = s_key + G * S + warp * kTallRingWords + half * kTallHalfWords;
-  int32_t *stage = reinterpret_cast<int32_t *>(s_key + G * S + nwarps * kTallRingWords) + warp * kTallStageWords;
-  int2 *sdc = reinterpret_cast<int2 *>(stage);          // slot x 10: (dist, count) of 8 targets
-  int2 *sdc2 = sdc + sl * 10;
-  int32_t *shp = stage + G * 10 * 2;                    // slot x 12: hop layers of 8 targets
-  int32_t *shp1 = shp + sl * 12;
+  uint32_t *ring = s_key + G * S + warp * tall_ring_words(RING) + half * tall_half_words(RING);
+  int32_t *stage = reinterpret_cast<int32_t *>(s_key + G * S + nwarps * tall_ring_words(RING)) + warp * kTallStageWords;
+  int2 *sdc = reinterpret_cast<int2 *>(stage);  // slot x 8 targets: (dist, count)
+  int2 *sdc2 = sdc + sl * 8;
+  int32_t *shp = stage + G * 8 * 2;             // slot x 8 targets: hop layer
+  int32_t *shp1 = shp + sl * 8;
   __shared__ int32_t s_h[G];
   __shared__ int64_t s_off[G];
   const int first = blockIdx.y * G;
@@ -671,9 +673,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
     int hiJ = have ? __ldg(hi + J) : 0x7fffffff;
     int loN = (have && J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
     uint32_t pending = 0;
+    int64_t toff_next = (4 * half < kend) ? a.lab_off[tb] : 0;
     for (int k = 0; k < 4; k++) {
       const int t = tb + k;
       const bool tv = 4 * half + k < kend;
+      const int64_t toff = toff_next;  // loaded one target ahead
+      toff_next = (k < 3 && 4 * half + k + 1 < kend) ? a.lab_off[t + 1] : 0;
       if (have && tv && k > 0) {  // advance the interval (targets grow by one)
         if (t >= hiJ) {
           do { J--; hiJ = __ldg(hi + J); } while (t >= hiJ);
@@ -690,25 +695,23 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
       for (int o = 8; o >= 1; o >>= 1) hh = max(hh, __shfl_xor_sync(kFull, hh, o));
       const int lim = (hh + 3) & ~3;  // entries of this half's target row to bring in
       const int nb = (max(hh, __shfl_xor_sync(kFull, hh, 16)) + kTallBlock - 1) / kTallBlock;
-      const int64_t toff = tv ? a.lab_off[t] : 0;
       const int32_t *trow = a.dis_sh + toff;
       auto issue = [&](int b) {  // block b of this half's row; an empty group past the last block
         if (b < nb) {
           const int e = b * kTallBlock + 4 * sl;
-          cp_async16(ring + (b % kTallRing) * kTallBlock + 4 * sl, e < lim ? trow + e : trow, e < lim);
+          cp_async16(ring + (b % RING) * kTallBlock + 4 * sl, e < lim ? trow + e : trow, e < lim);
         }
         cp_async_commit();
       };
       __syncwarp();  // the ring's slots are no longer read for the previous target
 #pragma unroll
-      for (int b = 0; b < kTallRing - 1; b++) issue(b);
+      for (int b = 0; b < RING - 1; b++) issue(b);
       uint32_t m1 = 0xffffffffu, m2 = 0xffffffffu, n1 = 0xffffffffu, n2 = 0xffffffffu;
       for (int b = 0; b < nb; b++) {
-        __syncwarp();  // block b - 1's slot is free
-        issue(b + kTallRing - 1);
-        cp_async_wait<kTallRing - 1>();  // this lane's part of block b has landed
-        __syncwarp();                     // and every lane's
-        const uint32_t *tbuf = ring + (b % kTallRing) * kTallBlock;
+        cp_async_wait<RING - 2>();  // this lane's part of block b has landed
+        __syncwarp();               // every lane's, and block b - 1 is no longer read
+        issue(b + RING - 1);        // into block b - 1's slot
+        const uint32_t *tbuf = ring + (b % RING) * kTallBlock;
         const uint32_t *xs = srow + b * kTallBlock;
         const int hm = min(hl - b * kTallBlock, kTallBlock);
         const int full8 = hm > 0 ? (hm & ~7) : 0;
@@ -765,12 +768,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
           hop = hx;
         }
       }
-      if (have && tv) {
-        sdc2[4 * half + k] = make_int2((int)dist, cnt);
+      if (have) {
+        sdc2[4 * half + k] = tv ? make_int2((int)dist, cnt) : make_int2(0, 0);
         if (COUNTS) shp1[4 * half + k] = hop;
-      } else if (have) {
-        sdc2[4 * half + k] = make_int2(0, 0);
-        if (COUNTS) shp1[4 * half + k] = 0;
       }
     }
     if (COUNTS && have && pending) {
@@ -799,13 +799,13 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
     {  // the warp's 16 slots x 8 targets are one contiguous block of records
       int4 *grec = a.out_rec + blk(first, t0, a.ns);
       for (int p = lane; p < gcount * 8; p += 32) {
-        const int2 x = sdc[(p >> 3) * 10 + (p & 7)];
+        const int2 x = sdc[p];
         grec[p] = make_int4(x.x, x.y, 0, 0);
       }
       if (COUNTS) {
         int4 *ghp = reinterpret_cast<int4 *>(a.out_hop + blk(first, t0, a.ns));
         const int4 *shp4 = reinterpret_cast<const int4 *>(shp);
-        for (int p = lane; p < gcount * 2; p += 32) ghp[p] = shp4[(p >> 1) * 3 + (p & 1)];
+        for (int p = lane; p < gcount * 2; p += 32) ghp[p] = shp4[p];
       }
     }
     __syncwarp();
@@ -1902,41 +1902,50 @@ static int tall_stride(const DeviceState *d) {
   if (((S / 4) & 1) == 0) S += 4;  // odd in 16-byte units: rows 0-7 start in distinct bank groups
   return S;
 }
-static int tall_warps(const Handle &h, const DeviceState *d) {
+// The configuration of the tall-tree kernel: warps (16, 12 or 8; the tuned label_warps when it
+// fits) and ring depth (4 blocks, else 3), the most warps first; {0, 0}: not used.
+struct TallCfg {
+  int warps, ring;
+};
+static TallCfg tall_cfg(const Handle &h, const DeviceState *d) {
   const Tuning &t = h.tuning;
-  if (t.label_sources == 32) return 0;
+  if (t.label_sources == 32) return {0, 0};
   if (t.label_sources == 0 &&
       (t.label_warps != 0 || t.label_tile > 0 || t.label_passes != 0 || packed_stride(h, d, 8) >= d->hmax_pad))
-    return 0;
-  const size_t budget = (size_t)std::max(0, d->smem_optin - 2048);
+    return {0, 0};
+  const size_t budget = (size_t)std::max(0, d->smem_optin - 1024);
+  const int S = tall_stride(d);
   const int w = t.label_warps;
-  if ((w == 8 || w == 12 || w == 16) && tall_smem(w, tall_stride(d)) <= budget) return w;
-  for (int x : {16, 12, 8})
-    if (tall_smem(x, tall_stride(d)) <= budget) return x;
-  return 0;
+  for (int x : {w, 16, 12, 8}) {
+    if (x != 8 && x != 12 && x != 16) continue;
+    for (int r : {4, 3})
+      if (tall_smem(x, r, S) <= budget) return {x, r};
+  }
+  return {0, 0};
 }
+static int tall_warps(const Handle &h, const DeviceState *d) { return tall_cfg(h, d).warps; }
 
-template <bool C, int W>
+template <bool C, int W, int R>
 static void launch_label_tall(const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
   const int S = tall_stride(d);
-  const size_t smem = tall_smem(W, S);
+  const size_t smem = tall_smem(W, R, S);
   const int groups = (ns + kTallSources - 1) / kTallSources;
   int split = std::max(1, (148 * 4 + groups - 1) / groups);
   split = std::min(split, std::max(1, (d->n_pad / 8) / W));
   a.stride = S;
   a.split = split;
-  CK(cudaFuncSetAttribute(k_label_scan_tall<C, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(k_label_scan_tall<C, W, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(split, groups);
-  k_label_scan_tall<C, W><<<grid, W * 32, smem, st>>>(a);
+  k_label_scan_tall<C, W, R><<<grid, W * 32, smem, st>>>(a);
   CK(cudaGetLastError());
 }
 
 template <bool C>
 static void launch_label_packed(const Handle &h, const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
-  const int tw = tall_warps(h, d);
-  if (tw == 16) return launch_label_tall<C, 16>(d, a, ns, st);
-  if (tw == 12) return launch_label_tall<C, 12>(d, a, ns, st);
-  if (tw == 8) return launch_label_tall<C, 8>(d, a, ns, st);
+  const TallCfg tc = tall_cfg(h, d);
+  if (tc.warps == 16) return tc.ring == 4 ? launch_label_tall<C, 16, 4>(d, a, ns, st) : launch_label_tall<C, 16, 3>(d, a, ns, st);
+  if (tc.warps == 12) return tc.ring == 4 ? launch_label_tall<C, 12, 4>(d, a, ns, st) : launch_label_tall<C, 12, 3>(d, a, ns, st);
+  if (tc.warps == 8) return tc.ring == 4 ? launch_label_tall<C, 8, 4>(d, a, ns, st) : launch_label_tall<C, 8, 3>(d, a, ns, st);
   const int w = packed_warps(h, d);
   if (w == 12) launch_label_pair<C>(h, d, a, ns, st);
   else if (w == 16) launch_label_packed_w<C, 16>(h, d, a, ns, st);
