@@ -293,7 +293,7 @@ def label_roofline(idx, shard, n, stats, steps, peak, peak_src, sm_mhz):
     achieved = dram_step / launches_step / (launch_ms / 1e3) / 1e9
     effective = algo_step / launches_step / (launch_ms / 1e3) / 1e9
     ent_per_clk = scan / (label_ms_step / 1e3) / (sm_mhz * 1e6) / 148.0
-    smem_roof = 256.0 / 6.0 if tall else 25.6
+    smem_roof = 32.0 if tall else 256.0 / 12.0
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "peak_source": peak_src,
             "kernel": "k_label_scan_tall" if tall else "k_label_scan_packed", "sources_per_cta": per_cta,
@@ -304,11 +304,13 @@ def label_roofline(idx, shard, n, stats, steps, peak, peak_src, sm_mhz):
                              "algorithmic_bytes_per_launch": algo_step / launches_step},
             "compute_roof": {"unit": "label entries/clk/SM", "achieved": ent_per_clk, "peak": smem_roof,
                              "frac": ent_per_clk / smem_roof, "issue_peak": 128.0 / 3.5,
-                             "note": ("tall-tree form: 6 shared-memory wavefronts per 256 lane-entries (two "
-                                      "targets per warp, 16 source rows per load: 42.7)" if tall else
-                                      "5 shared-memory wavefronts per 128 lane-entries (25.6)") +
-                                     " and 3.5 instructions per pair-entry at 128 lane-instructions/clk/SM "
-                                     "(issue_peak)"},
+                             "note": "shared-memory roof: a 16-byte shared load takes at least one wavefront "
+                                     "per half-warp (2 for a full-warp broadcast, measured); " +
+                                     ("tall-tree form: lane pairs share a source row, so 8 wavefronts per 8 "
+                                      "entries of 32 pairs (32.0)" if tall else
+                                      "32 distinct source rows + broadcast target: 12 wavefronts per 8 entries "
+                                      "of 32 pairs (21.3)") +
+                                     "; issue_peak: 3.5 instructions per pair-entry at 128 lane-instructions/clk/SM"},
             "note": "frac = modelled DRAM bytes per launch / launch time / measured HBM copy bandwidth; traffic "
                     "is not measured in this run (ncu figures for the same kernel are in profiles/)"}
 

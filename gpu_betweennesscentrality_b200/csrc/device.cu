@@ -577,19 +577,23 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_packed(LabelArgs a
 // ------------------------------------------------------------------------------- K1 + K2, tall trees
 // Packed-key label scan for trees too tall for the 32-source CTA to hold its source rows in shared
 // memory (MHLQBC.cu:379-392 is the scan it replaces).  A CTA takes 16 sources, so whole rows fit
-// (16 x height x 4 bytes: 175 KB at height 2,728).  Each warp scans two targets at once: lanes
-// 0-15 pair the 16 sources with target A, lanes 16-31 with target B, so one 16-byte shared load of
-// the source keys serves both halves (16 distinct rows: 2 wavefronts instead of 4 for 32 rows) and
-// each half's target row is a broadcast.  Target rows stream through a per-half ring of RING blocks
-// of 64 entries filled by cp.async (16 bytes per lane, RING - 1 blocks ahead of the scan, only up
-// to the half's deepest LCA), so no entry of a scan is read from global memory.  Keys, tie
-// detection, count/hop gathers and the chunk-blocked output are those of k_label_scan_packed.
+// (16 x height x 4 bytes: 175 KB at height 2,728).  Each warp scans two targets at once: lane l
+// pairs source l / 2 with target A (even lanes) or B (odd lanes).  A 16-byte shared load is served
+// per half-warp, at least one wavefront each (measured on B200: a broadcast to all 32 lanes costs
+// 2, 16 distinct rows per half-warp cost 2 per half); with the lane pairs of a half-warp sharing a
+// source row, each half-warp reads 8 source rows (one wavefront) and the two targets' rows (one
+// wavefront, the two rings in different bank groups): 8 wavefronts per 8 entries of 32 pairs,
+// against 12 for 32 distinct source rows.  Target rows stream through a per-target ring of RING
+// blocks of 64 entries filled by cp.async (16 bytes per lane, RING - 1 blocks ahead of the scan,
+// only up to the deepest LCA of that target's pairs), so no entry of a scan is read from global
+// memory.  Keys, tie detection, count/hop gathers and the chunk-blocked output are those of
+// k_label_scan_packed.
 // (Measured: 16 warps with a 3-block ring beat 12 warps with 4 at 1M, 9.3 vs 8.7 entries/clk/SM;
 // one stream over a chunk's four targets, instead of a ring refilled per target, was slower:
 // its per-block bookkeeping cost more than the latency it hid.)
 constexpr int kTallSources = 16;
 constexpr int kTallBlock = 64;  // entries per block (16 lanes x 4)
-__host__ __device__ constexpr int tall_half_words(int ring) { return ring * kTallBlock + 4; }  // +4: halves in different bank groups
+__host__ __device__ constexpr int tall_half_words(int ring) { return ring * kTallBlock + 4; }  // +4: the two rings in different bank groups
 __host__ __device__ constexpr int tall_ring_words(int ring) { return 2 * tall_half_words(ring); }  // per warp
 constexpr int kTallStageWords = kTallSources * 8 * 2 + kTallSources * 8;  // per warp: (dist, count) and hop of 16 x 8 pairs
 
@@ -613,8 +617,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
   uint32_t *s_key = reinterpret_cast<uint32_t *>(smem4);
   const int S = a.stride;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  const int half = lane >> 4, sl = lane & 15;
-  uint32_t *ring = s_key + G * S + warp * tall_ring_words(RING) + half * tall_half_words(RING);
+  const int side = lane & 1, sl = lane >> 1;  // target side (A, B) and source slot of this lane
+  uint32_t *ring = s_key + G * S + warp * tall_ring_words(RING) + side * tall_half_words(RING);
   int32_t *stage = reinterpret_cast<int32_t *>(s_key + G * S + nwarps * tall_ring_words(RING)) + warp * kTallStageWords;
   int2 *sdc = reinterpret_cast<int2 *>(stage);  // slot x 8 targets: (dist, count)
   int2 *sdc2 = sdc + sl * 8;
@@ -656,7 +660,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
   for (int c = cbeg + warp; c < cend; c += nwarps) {
     const int t0 = c << 3;
     const int kend = min(8, a.n - t0);
-    const int tb = t0 + 4 * half;  // this half's targets: tb .. tb + 3
+    const int tb = t0 + 4 * side;  // this side's targets: tb .. tb + 3
     // deepest ancestor interval of this lane's source holding tb (binary search)
     int J = 0;
     if (tb < a.n) {
@@ -673,12 +677,12 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
     int hiJ = have ? __ldg(hi + J) : 0x7fffffff;
     int loN = (have && J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
     uint32_t pending = 0;
-    int64_t toff_next = (4 * half < kend) ? a.lab_off[tb] : 0;
+    int64_t toff_next = (4 * side < kend) ? a.lab_off[tb] : 0;
     for (int k = 0; k < 4; k++) {
       const int t = tb + k;
-      const bool tv = 4 * half + k < kend;
+      const bool tv = 4 * side + k < kend;
       const int64_t toff = toff_next;  // loaded one target ahead
-      toff_next = (k < 3 && 4 * half + k + 1 < kend) ? a.lab_off[t + 1] : 0;
+      toff_next = (k < 3 && 4 * side + k + 1 < kend) ? a.lab_off[t + 1] : 0;
       if (have && tv && k > 0) {  // advance the interval (targets grow by one)
         if (t >= hiJ) {
           do { J--; hiJ = __ldg(hi + J); } while (t >= hiJ);
@@ -690,13 +694,13 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
         }
       }
       const int hl = (have && tv) ? J + 1 : 0;
-      int hh = hl;  // the half's deepest scan, then the warp's
+      int hh = hl;  // the side's deepest scan (lanes of one parity), then the warp's
 #pragma unroll
-      for (int o = 8; o >= 1; o >>= 1) hh = max(hh, __shfl_xor_sync(kFull, hh, o));
-      const int lim = (hh + 3) & ~3;  // entries of this half's target row to bring in
-      const int nb = (max(hh, __shfl_xor_sync(kFull, hh, 16)) + kTallBlock - 1) / kTallBlock;
+      for (int o = 16; o >= 2; o >>= 1) hh = max(hh, __shfl_xor_sync(kFull, hh, o));
+      const int lim = (hh + 3) & ~3;  // entries of this side's target row to bring in
+      const int nb = (max(hh, __shfl_xor_sync(kFull, hh, 1)) + kTallBlock - 1) / kTallBlock;
       const int32_t *trow = a.dis_sh + toff;
-      auto issue = [&](int b) {  // block b of this half's row; an empty group past the last block
+      auto issue = [&](int b) {  // block b of this side's row; an empty group past the last block
         if (b < nb) {
           const int e = b * kTallBlock + 4 * sl;
           cp_async16(ring + (b % RING) * kTallBlock + 4 * sl, e < lim ? trow + e : trow, e < lim);
@@ -769,8 +773,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
         }
       }
       if (have) {
-        sdc2[4 * half + k] = tv ? make_int2((int)dist, cnt) : make_int2(0, 0);
-        if (COUNTS) shp1[4 * half + k] = hop;
+        sdc2[4 * side + k] = tv ? make_int2((int)dist, cnt) : make_int2(0, 0);
+        if (COUNTS) shp1[4 * side + k] = hop;
       }
     }
     if (COUNTS && have && pending) {
@@ -778,7 +782,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         if (pending & (1u << k)) {
-          const int jm = sdc2[4 * half + k].y;
+          const int jm = sdc2[4 * side + k].y;
           cs4[k] = __ldg(a.ch + soff + jm);
           ct4[k] = __ldg(a.ch + a.lab_off[tb + k] + jm);
         }
@@ -786,14 +790,14 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
 #pragma unroll
       for (int k = 0; k < 4; k++) {
         if (pending & (1u << k)) {
-          sdc2[4 * half + k].y = (int)((unsigned)cs4[k].x * (unsigned)ct4[k].x);
-          shp1[4 * half + k] = cs4[k].y + ct4[k].y;
+          sdc2[4 * side + k].y = (int)((unsigned)cs4[k].x * (unsigned)ct4[k].x);
+          shp1[4 * side + k] = cs4[k].y + ct4[k].y;
         }
       }
     }
     if (COUNTS && have) {
 #pragma unroll
-      for (int k = 0; k < 4; k++) mh = max(mh, shp1[4 * half + k]);
+      for (int k = 0; k < 4; k++) mh = max(mh, shp1[4 * side + k]);
     }
     __syncwarp();
     {  // the warp's 16 slots x 8 targets are one contiguous block of records
