@@ -165,13 +165,14 @@ class Index:
         return int(g[0])
 
     TUNING_KEYS = ("lanes_per_source", "label_threads", "split", "chunk", "dep_threads", "dep_form", "queue_depth",
-                   "label_warps", "label_tile", "label_passes", "sweep_delta", "sweep_threads", "label_sources")
+                   "label_warps", "label_tile", "label_passes", "sweep_delta", "sweep_threads", "label_sources",
+                   "label_stream")
 
     def set_tuning(self, lanes_per_source=0, label_threads=256, split=0, chunk=0, dep_threads=256, dep_form=0,
                    queue_depth=0, label_warps=0, label_tile=0, label_passes=0, sweep_delta=0, sweep_threads=0,
-                   label_sources=0):
+                   label_sources=0, label_stream=0):
         p = i32([lanes_per_source, label_threads, split, chunk, dep_threads, dep_form, queue_depth, label_warps,
-                 label_tile, label_passes, sweep_delta, sweep_threads, label_sources])
+                 label_tile, label_passes, sweep_delta, sweep_threads, label_sources, label_stream])
         check(lib().qbc_index_set_tuning(self.h, ptr(p, i32p), len(self.TUNING_KEYS)))
 
     def get_tuning(self):

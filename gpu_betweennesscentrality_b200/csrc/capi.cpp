@@ -47,7 +47,7 @@ void need(bool ok, const char *what) {
   if (!ok) throw qbc::Error(QBC_EINVAL, what);
 }
 
-constexpr int32_t kTuningFields = 13;  // qbc_index_set_tuning's params layout
+constexpr int32_t kTuningFields = 14;  // qbc_index_set_tuning's params layout
 
 void not_serving(const qbc_index *idx) {
   if (idx->h.server) throw qbc::Error(QBC_EBUSY, "the index is serving requests: close its server first");
@@ -271,7 +271,7 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
     need(idx && (nparams == 0 || params), "null argument");
     qbc::Tuning &t = idx->h.tuning;
     not_serving(idx);
-    int32_t *f[] = {&t.lanes_per_source, &t.label_threads, &t.split, &t.chunk, &t.dep_threads, &t.dep_form, &t.queue_depth, &t.label_warps, &t.label_tile, &t.label_passes, &t.sweep_delta, &t.sweep_threads, &t.label_sources};
+    int32_t *f[] = {&t.lanes_per_source, &t.label_threads, &t.split, &t.chunk, &t.dep_threads, &t.dep_form, &t.queue_depth, &t.label_warps, &t.label_tile, &t.label_passes, &t.sweep_delta, &t.sweep_threads, &t.label_sources, &t.label_stream};
     if (nparams > 0) {
       int32_t k = params[0];
       need(k == 0 || k == 1 || k == 2 || k == 4 || k == 8 || k == 16 || k == 32, "lanes per source must be 0 or a power of two <= 32");
@@ -288,6 +288,7 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
     if (nparams > 11)
       need(params[11] == 0 || params[11] == 256 || params[11] == 512 || params[11] == 1024, "sweep threads must be 0, 256, 512 or 1024");
     if (nparams > 12) need(params[12] == 0 || params[12] == 16 || params[12] == 32, "label sources must be 0, 16 or 32");
+    if (nparams > 13) need(params[13] >= 0 && params[13] <= 2, "label stream must be 0, 1 or 2");
     for (int32_t i = 0; i < nparams && i < kTuningFields; i++) *f[i] = params[i];
     if (nparams > 3 && t.chunk != old_chunk && idx->h.dev) qbc::device_set_chunk(idx->h, t.chunk);
   });
@@ -297,7 +298,7 @@ int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams)
   return guarded([&] {
     need(idx && (nparams == 0 || params), "null argument");
     const qbc::Tuning &t = idx->h.tuning;
-    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes, t.sweep_delta, t.sweep_threads, t.label_sources};
+    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes, t.sweep_delta, t.sweep_threads, t.label_sources, t.label_stream};
     for (int32_t i = 0; i < nparams && i < kTuningFields; i++) params[i] = f[i];
   });
 }
@@ -386,7 +387,7 @@ int qbc_autotune(qbc_index *idx, const int32_t *sources0, int32_t ns, int32_t *p
     qbc::autotune(idx->h, sources0, ns, &ms);
     if (ms_per_source) *ms_per_source = ms;
     const qbc::Tuning &t = idx->h.tuning;
-    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes, t.sweep_delta, t.sweep_threads, t.label_sources};
+    const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.chunk, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes, t.sweep_delta, t.sweep_threads, t.label_sources, t.label_stream};
     for (int32_t i = 0; params && i < nparams && i < kTuningFields; i++) params[i] = f[i];
   });
 }

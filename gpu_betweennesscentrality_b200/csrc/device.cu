@@ -64,6 +64,7 @@ struct LabelArgs {
   int32_t pass_lo;                   // multi-pass packed kernel: first row entry of this pass's tile
   int32_t multipass;                 // launcher only: rows longer than the tile take several passes
                                      // (kernel variant MP, state in out_rec between passes)
+  int32_t row_words;                 // lane-pair kernel: words per target-row buffer
   int32_t *err;                      // device error word (packed kernel's bounded waits)
   uint32_t wait_spins;               // attempts of a row-copy wait before it is reported
 };
@@ -785,6 +786,232 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_tall(LabelArgs a) 
           const int jm = sdc2[4 * side + k].y;
           cs4[k] = __ldg(a.ch + soff + jm);
           ct4[k] = __ldg(a.ch + a.lab_off[tb + k] + jm);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (pending & (1u << k)) {
+          sdc2[4 * side + k].y = (int)((unsigned)cs4[k].x * (unsigned)ct4[k].x);
+          shp1[4 * side + k] = cs4[k].y + ct4[k].y;
+        }
+      }
+    }
+    if (COUNTS && have) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) mh = max(mh, shp1[4 * side + k]);
+    }
+    __syncwarp();
+    {  // the warp's 16 slots x 8 targets are one contiguous block of records
+      int4 *grec = a.out_rec + blk(first, t0, a.ns);
+      for (int p = lane; p < gcount * 8; p += 32) {
+        const int2 x = sdc[p];
+        grec[p] = make_int4(x.x, x.y, 0, 0);
+      }
+      if (COUNTS) {
+        int4 *ghp = reinterpret_cast<int4 *>(a.out_hop + blk(first, t0, a.ns));
+        const int4 *shp4 = reinterpret_cast<const int4 *>(shp);
+        for (int p = lane; p < gcount * 2; p += 32) ghp[p] = shp4[p];
+      }
+    }
+    __syncwarp();
+  }
+  cp_async_wait<0>();
+  if (COUNTS && have && a.maxhop) atomicMax(a.maxhop + first + sl, mh);
+}
+
+// ------------------------------------------------------------------------------- K1 + K2, lane pairs
+// The lane-pair layout of k_label_scan_tall for trees whose whole rows fit twice per warp side:
+// 16 sources per CTA, lane l pairs source l / 2 with target A or B (8 shared-memory wavefronts per
+// 8 entries of 32 pairs), and each side's target row is copied whole by cp.async into a per-side
+// double buffer while the previous target is scanned (the next target's LCA depth is known ahead:
+// the four targets of a side are consecutive, so their depths come from one interval walk).  The
+// tie re-scan reads the target row from the buffer.
+template <class T>
+__device__ __forceinline__ T pick4(const T (&x)[4], int k) {  // x[k] without dynamic register indexing
+  return k == 0 ? x[0] : k == 1 ? x[1] : k == 2 ? x[2] : x[3];
+}
+
+__host__ __device__ constexpr int rows16_side_words(int R) { return 2 * R + 4; }  // +4: the sides in different bank groups
+__host__ __device__ constexpr size_t rows16_smem(int warps, int S, int R) {
+  return (size_t)kTallSources * S * 4 + (size_t)warps * (2 * rows16_side_words(R) + kTallStageWords) * 4;
+}
+
+template <bool COUNTS, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 1) k_label_scan_rows16(LabelArgs a) {
+  constexpr int G = kTallSources;
+  extern __shared__ int4 smem4[];
+  uint32_t *s_key = reinterpret_cast<uint32_t *>(smem4);
+  const int S = a.stride, R = a.row_words;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int side = lane & 1, sl = lane >> 1;  // target side (A, B) and source slot of this lane
+  uint32_t *rbuf = s_key + G * S + warp * 2 * rows16_side_words(R) + side * rows16_side_words(R);
+  int32_t *stage = reinterpret_cast<int32_t *>(s_key + G * S + nwarps * 2 * rows16_side_words(R)) + warp * kTallStageWords;
+  int2 *sdc = reinterpret_cast<int2 *>(stage);  // slot x 8 targets: (dist, count)
+  int2 *sdc2 = sdc + sl * 8;
+  int32_t *shp = stage + G * 8 * 2;             // slot x 8 targets: hop layer
+  int32_t *shp1 = shp + sl * 8;
+  __shared__ int32_t s_h[G];
+  __shared__ int64_t s_off[G];
+  const int first = blockIdx.y * G;
+  if (first >= a.ns) return;
+  const int gcount = min(G, a.ns - first);
+  const uint32_t B = (uint32_t)a.bits, mask = (1u << B) - 1u;
+  if (threadIdx.x < G) {
+    const int i = threadIdx.x;
+    const int s = i < gcount ? a.src[first + i] : 0;
+    s_h[i] = i < gcount ? a.depth[s] : 0;
+    s_off[i] = a.lab_off[s];
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < G * S; idx += blockDim.x) {
+    const int i = idx / S, j = idx - i * S;
+    uint32_t key = 0xffffffffu;
+    if (i < gcount && j < s_h[i]) key = (uint32_t)a.dis_sh[s_off[i] + j] | (uint32_t)j;
+    s_key[idx] = key;
+  }
+  __syncthreads();
+
+  const bool have = sl < gcount;
+  const int hs = have ? s_h[sl] : 1;
+  const int64_t soff = s_off[sl];
+  const uint32_t *srow = s_key + sl * S;
+  const int32_t *lo = a.src_rows + (size_t)(first + (have ? sl : 0)) * 2 * a.src_stride;
+  const int32_t *hi = lo + a.src_stride;
+  const int nsteps = 32 - __clz(hs);
+  int mh = 0;
+
+  const int nchunk = a.n_pad >> 3;
+  const int cbeg = (int)((int64_t)nchunk * blockIdx.x / a.split);
+  const int cend = (int)((int64_t)nchunk * (blockIdx.x + 1) / a.split);
+  for (int c = cbeg + warp; c < cend; c += nwarps) {
+    const int t0 = c << 3;
+    const int kend = min(8, a.n - t0);
+    const int tb = t0 + 4 * side;  // this side's targets: tb .. tb + 3
+    int hl[4], lim[4];
+    int64_t toff[4];
+    {  // LCA depths of this lane's source with the side's four targets (one interval walk)
+      int J = 0;
+      if (tb < a.n) {
+        int h = have ? hs : 1;
+        for (int it = 0; it < nsteps; it++) {
+          if (h - J > 1) {
+            const int mid = (J + h) >> 1;
+            const bool p = (__ldg(lo + mid) <= tb) && (tb < __ldg(hi + mid));
+            J = p ? mid : J;
+            h = p ? h : mid;
+          }
+        }
+      }
+      int hiJ = have ? __ldg(hi + J) : 0x7fffffff;
+      int loN = (have && J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int t = tb + k;
+        const bool tv = 4 * side + k < kend;
+        toff[k] = tv ? a.lab_off[t] : 0;
+        if (have && tv && k > 0) {
+          if (t >= hiJ) {
+            do { J--; hiJ = __ldg(hi + J); } while (t >= hiJ);
+            loN = __ldg(lo + J + 1);
+          } else if (t == loN) {
+            J++;
+            hiJ = __ldg(hi + J);
+            loN = (J + 1 < hs) ? __ldg(lo + J + 1) : 0x7fffffff;
+          }
+        }
+        hl[k] = (have && tv) ? J + 1 : 0;
+        int hh = hl[k];  // the side's deepest scan (lanes of one parity)
+#pragma unroll
+        for (int o = 16; o >= 2; o >>= 1) hh = max(hh, __shfl_xor_sync(kFull, hh, o));
+        lim[k] = (hh + 3) & ~3;
+      }
+    }
+    auto issue_row = [&](int k) {  // the side's row of target k, whole, into buffer k & 1
+      const int lk = pick4(lim, k);
+      const int32_t *trow = a.dis_sh + pick4(toff, k);
+      uint32_t *dst = rbuf + (k & 1) * R;
+      for (int e = 4 * sl; e < lk; e += 64) cp_async16(dst + e, trow + e, true);
+      cp_async_commit();
+    };
+    uint32_t pending = 0;
+    __syncwarp();  // the buffers are no longer read for the previous chunk
+    issue_row(0);
+    for (int k = 0; k < 4; k++) {
+      if (k < 3) issue_row(k + 1);  // into the buffer target k - 1 used
+      else cp_async_commit();
+      cp_async_wait<1>();  // this lane's pieces of target k's row have landed
+      __syncwarp();        // and every lane's
+      const int hlk = pick4(hl, k);
+      const uint32_t *tbuf = rbuf + (k & 1) * R;
+      uint32_t m1 = 0xffffffffu, m2 = 0xffffffffu, n1 = 0xffffffffu, n2 = 0xffffffffu;
+      const int full8 = hlk & ~7;
+      int j = 0;
+      for (; j < full8; j += 8) {
+        const uint4 x = *reinterpret_cast<const uint4 *>(srow + j);
+        const uint4 y = *reinterpret_cast<const uint4 *>(tbuf + j);
+        const uint4 x2 = *reinterpret_cast<const uint4 *>(srow + j + 4);
+        const uint4 y2 = *reinterpret_cast<const uint4 *>(tbuf + j + 4);
+        const uint32_t v0 = x.x + y.x, v1 = x.y + y.y, v2 = x.z + y.z, v3 = x.w + y.w;
+        const uint32_t u0 = x2.x + y2.x, u1 = x2.y + y2.y, u2 = x2.z + y2.z, u3 = x2.w + y2.w;
+        m1 = __vimin3_u32(m1, v0, v1);
+        n1 = __vimin3_u32(n1, u0, u1);
+        m1 = __vimin3_u32(m1, v2, v3);
+        n1 = __vimin3_u32(n1, u2, u3);
+        m2 = __vimin3_u32(m2, v0 ^ mask, v1 ^ mask);
+        n2 = __vimin3_u32(n2, u0 ^ mask, u1 ^ mask);
+        m2 = __vimin3_u32(m2, v2 ^ mask, v3 ^ mask);
+        n2 = __vimin3_u32(n2, u2 ^ mask, u3 ^ mask);
+      }
+      for (; j < hlk; j += 4) {
+        const uint4 x = *reinterpret_cast<const uint4 *>(srow + j);
+        const uint4 y = *reinterpret_cast<const uint4 *>(tbuf + j);
+        const uint32_t v0 = x.x + y.x;
+        const uint32_t v1 = (j + 1 < hlk) ? x.y + y.y : 0xffffffffu;
+        const uint32_t v2 = (j + 2 < hlk) ? x.z + y.z : 0xffffffffu;
+        const uint32_t v3 = (j + 3 < hlk) ? x.w + y.w : 0xffffffffu;
+        m1 = __vimin3_u32(m1, v0, v1);
+        m1 = __vimin3_u32(m1, v2, v3);
+        m2 = __vimin3_u32(m2, v0 ^ mask, (j + 1 < hlk) ? v1 ^ mask : 0xffffffffu);
+        m2 = __vimin3_u32(m2, (j + 2 < hlk) ? v2 ^ mask : 0xffffffffu, (j + 3 < hlk) ? v3 ^ mask : 0xffffffffu);
+      }
+      m1 = min(m1, n1);
+      m2 = min(m2, n2);
+      const bool tv = hlk > 0;
+      const uint32_t dist = m1 >> B;
+      int cnt = 0, hop = 0;
+      if (COUNTS && tv) {
+        if ((m1 ^ m2) == mask) {
+          cnt = (int)(m1 & mask);  // the minimising entry; counts resolved after the chunk
+          pending |= 1u << k;
+        } else {  // a tie: sum over every minimising entry
+          const int64_t tk = pick4(toff, k);
+          unsigned cc = 0;
+          int hx = 0;
+          for (int q = 0; q < hlk; q++) {
+            if (((srow[q] + tbuf[q]) >> B) == dist) {
+              const int2 cs = __ldg(a.ch + soff + q), ct = __ldg(a.ch + tk + q);
+              cc += (unsigned)cs.x * (unsigned)ct.x;
+              hx = max(hx, cs.y + ct.y);
+            }
+          }
+          cnt = (int)cc;
+          hop = hx;
+        }
+      }
+      if (have) {
+        sdc2[4 * side + k] = tv ? make_int2((int)dist, cnt) : make_int2(0, 0);
+        if (COUNTS) shp1[4 * side + k] = hop;
+      }
+      __syncwarp();  // target k's buffer is free for target k + 2
+    }
+    if (COUNTS && have && pending) {
+      int2 cs4[4], ct4[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (pending & (1u << k)) {
+          const int jm = sdc2[4 * side + k].y;
+          cs4[k] = __ldg(a.ch + soff + jm);
+          ct4[k] = __ldg(a.ch + toff[k] + jm);
         }
       }
 #pragma unroll
@@ -1906,26 +2133,36 @@ static int tall_stride(const DeviceState *d) {
   if (((S / 4) & 1) == 0) S += 4;  // odd in 16-byte units: rows 0-7 start in distinct bank groups
   return S;
 }
-// The configuration of the tall-tree kernel: warps (16, 12 or 8; the tuned label_warps when it
-// fits) and ring depth (4 blocks, else 3), the most warps first; {0, 0}: not used.
+// The configuration of the 16-source kernels: whole target rows (k_label_scan_rows16) or a ring of
+// 64-entry blocks (k_label_scan_tall); warps 16, 12 or 8 (the tuned label_warps when it fits), the
+// ring 4 blocks deep, else 3; {0, ...}: the 32-source kernels.  Auto: the 16-source kernels when
+// the 32-source kernel cannot hold whole rows and its warps, tile and passes are not tuned; whole
+// rows when they fit with 16 warps.
 struct TallCfg {
   int warps, ring;
+  bool whole;
 };
+static int rows16_words(const DeviceState *d) { return d->hmax_pad; }
 static TallCfg tall_cfg(const Handle &h, const DeviceState *d) {
   const Tuning &t = h.tuning;
-  if (t.label_sources == 32) return {0, 0};
+  if (t.label_sources == 32) return {0, 0, false};
   if (t.label_sources == 0 &&
       (t.label_warps != 0 || t.label_tile > 0 || t.label_passes != 0 || packed_stride(h, d, 8) >= d->hmax_pad))
-    return {0, 0};
+    return {0, 0, false};
   const size_t budget = (size_t)std::max(0, d->smem_optin - 1024);
-  const int S = tall_stride(d);
+  const int S = tall_stride(d), R = rows16_words(d);
   const int w = t.label_warps;
+  auto fits_whole = [&](int x) { return rows16_smem(x, S, R) <= budget; };
+  if (t.label_stream == 1 || (t.label_stream == 0 && fits_whole(16))) {
+    for (int x : {w, 16, 12, 8})
+      if ((x == 8 || x == 12 || x == 16) && fits_whole(x)) return {x, 0, true};
+  }
   for (int x : {w, 16, 12, 8}) {
     if (x != 8 && x != 12 && x != 16) continue;
     for (int r : {4, 3})
-      if (tall_smem(x, r, S) <= budget) return {x, r};
+      if (tall_smem(x, r, S) <= budget) return {x, r, false};
   }
-  return {0, 0};
+  return {0, 0, false};
 }
 static int tall_warps(const Handle &h, const DeviceState *d) { return tall_cfg(h, d).warps; }
 
@@ -1944,9 +2181,30 @@ static void launch_label_tall(const DeviceState *d, LabelArgs a, int32_t ns, cud
   CK(cudaGetLastError());
 }
 
+template <bool C, int W>
+static void launch_label_rows16(const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
+  const int S = tall_stride(d), R = rows16_words(d);
+  const size_t smem = rows16_smem(W, S, R);
+  const int groups = (ns + kTallSources - 1) / kTallSources;
+  int split = std::max(1, (148 * 4 + groups - 1) / groups);
+  split = std::min(split, std::max(1, (d->n_pad / 8) / W));
+  a.stride = S;
+  a.row_words = R;
+  a.split = split;
+  CK(cudaFuncSetAttribute(k_label_scan_rows16<C, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(split, groups);
+  k_label_scan_rows16<C, W><<<grid, W * 32, smem, st>>>(a);
+  CK(cudaGetLastError());
+}
+
 template <bool C>
 static void launch_label_packed(const Handle &h, const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
   const TallCfg tc = tall_cfg(h, d);
+  if (tc.whole) {
+    if (tc.warps == 16) return launch_label_rows16<C, 16>(d, a, ns, st);
+    if (tc.warps == 12) return launch_label_rows16<C, 12>(d, a, ns, st);
+    return launch_label_rows16<C, 8>(d, a, ns, st);
+  }
   if (tc.warps == 16) return tc.ring == 4 ? launch_label_tall<C, 16, 4>(d, a, ns, st) : launch_label_tall<C, 16, 3>(d, a, ns, st);
   if (tc.warps == 12) return tc.ring == 4 ? launch_label_tall<C, 12, 4>(d, a, ns, st) : launch_label_tall<C, 12, 3>(d, a, ns, st);
   if (tc.warps == 8) return tc.ring == 4 ? launch_label_tall<C, 8, 4>(d, a, ns, st) : launch_label_tall<C, 8, 3>(d, a, ns, st);

@@ -24,6 +24,8 @@ struct Tuning {
   int32_t sweep_threads = 0;     // CSR index: threads per CTA of the sweep (256, 512 or 1024; 0 = 512)
   int32_t label_sources = 0;     // packed-key label kernel: sources per CTA (32, or 16 with whole rows of
                                  // tall trees in shared memory); 0 = auto
+  int32_t label_stream = 0;      // 16-source kernel: 1 whole target rows double-buffered, 2 64-entry
+                                 // blocks through a ring; 0 = auto (whole rows when they fit 16 warps)
 };
 
 struct DeviceState;  // opaque, defined in device_state.h

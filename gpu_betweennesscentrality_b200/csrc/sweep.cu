@@ -60,7 +60,7 @@ uint64_t fnv(uint64_t h, const void *p, size_t bytes) {
 
 uint64_t tuning_key(const Handle &h, const DeviceState *d) {
   const Tuning &t = h.tuning;
-  const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes, t.sweep_delta, t.sweep_threads, t.label_sources, d->chunk};
+  const int32_t f[] = {t.lanes_per_source, t.label_threads, t.split, t.dep_threads, t.dep_form, t.queue_depth, t.label_warps, t.label_tile, t.label_passes, t.sweep_delta, t.sweep_threads, t.label_sources, t.label_stream, d->chunk};
   return fnv(1469598103934665603ull, f, sizeof(f));
 }
 
@@ -351,8 +351,9 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
       return;
     }
     // 1. label kernel: the packed-key kernel with 32 sources per CTA and 8-20 warps (0 lanes) and,
-    //    for tall trees, tile passes or a global-memory tail; its 16-source form (whole rows in
-    //    shared memory, two targets per warp) with 8, 12 or 16 warps; or the general kernel with
+    //    for tall trees, tile passes or a global-memory tail; its 16-source forms (whole source rows
+    //    in shared memory, two targets per warp; target rows whole or through a ring) with 8, 12 or
+    //    16 warps; or the general kernel with
     //    32/K sources per CTA and 128 or 256 threads
     if (d->packed_bits) {
       for (int32_t warps : {8, 12, 16, 20})  // 12: the two-target kernel
@@ -365,15 +366,17 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
           t.label_passes = passes;
           trial(t);
         }
-      for (int32_t warps : {8, 12, 16}) {
-        Tuning t = best;
-        t.lanes_per_source = 0;
-        t.label_sources = 16;
-        t.label_warps = warps;
-        t.label_passes = 0;
-        t.label_tile = 0;
-        trial(t);
-      }
+      for (int32_t stream : {1, 2})
+        for (int32_t warps : {8, 12, 16}) {
+          Tuning t = best;
+          t.lanes_per_source = 0;
+          t.label_sources = 16;
+          t.label_stream = stream;
+          t.label_warps = warps;
+          t.label_passes = 0;
+          t.label_tile = 0;
+          trial(t);
+        }
     }
     for (int32_t lanes : {4, 8, 16})
       for (int32_t threads : {128, 256}) {

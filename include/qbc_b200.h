@@ -133,8 +133,10 @@ int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int3
  * mean arc weight), [11]=threads per CTA of that sweep (256, 512 or 1024; 0 = 512), [12]=sources
  * per CTA of the packed-key label scan (32; 16 = the tall-tree kernel: whole rows of 16 sources in
  * shared memory, two targets per warp, target rows streamed through a cp.async ring, when the
- * height fits; 0 = auto: 16 when the 32-source kernel cannot hold whole rows and [7]-[9] are 0).
- * Refused with QBC_EBUSY while the index serves. */
+ * height fits; 0 = auto: 16 when the 32-source kernel cannot hold whole rows and [7]-[9] are 0),
+ * [13]=target rows of the 16-source kernel (1 = whole rows, double-buffered per warp side; 2 =
+ * 64-entry blocks through a ring; 0 = auto: whole rows when they fit with 16 warps).  Refused
+ * with QBC_EBUSY while the index serves. */
 int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams);
 int qbc_index_get_tuning(const qbc_index *idx, int32_t *params, int32_t nparams);
 

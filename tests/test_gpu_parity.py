@@ -80,18 +80,19 @@ def test_packed_kernel_tiles_and_warps(g2k, warps, tile, passes):
     assert rel_err(bc, tc.bc(arcs, srcs)) <= BC_RTOL
 
 
-@pytest.mark.parametrize("warps", [0, 8, 12, 16])
-def test_tall_tree_kernel_forced_2k(g2k, warps):
-    """the tall-tree form of the packed scan (16 sources per CTA, two targets per warp, target rows
-    through a cp.async ring) forced on the 2k graph: a ragged last group of sources, target chunks
-    cut by n, ties -- rows bit-identical to the 32-source kernel's, BC against the oracle"""
+@pytest.mark.parametrize("warps,stream", [(0, 0), (8, 1), (12, 1), (16, 1), (8, 2), (12, 2), (16, 2)])
+def test_tall_tree_kernel_forced_2k(g2k, warps, stream):
+    """the 16-source forms of the packed scan (lane pairs: two targets per warp; target rows whole
+    and double-buffered, or in 64-entry blocks through a cp.async ring) forced on the 2k graph: a
+    ragged last group of sources, target chunks cut by n, ties -- rows bit-identical to the
+    32-source kernel's, BC against the oracle"""
     n, u, v, w, g, idx, tc, arcs = g2k
     srcs = np.arange(3, n, 11, dtype=np.int32)  # 182 sources: 11 groups of 16 and one of 6
     idx.set_tuning(label_sources=32)
     try:
         assert idx.label_group() == 32
         base = idx.rows(srcs)
-        idx.set_tuning(label_sources=16, label_warps=warps)
+        idx.set_tuning(label_sources=16, label_warps=warps, label_stream=stream)
         assert idx.label_group() == 16
         alt = idx.rows(srcs)
         bc = idx.bc_sources(srcs)
@@ -102,7 +103,8 @@ def test_tall_tree_kernel_forced_2k(g2k, warps):
     assert rel_err(bc, tc.bc(arcs, srcs)) <= BC_RTOL
 
 
-def test_tall_tree_kernel_unit_weight_ties():
+@pytest.mark.parametrize("stream", [1, 2])
+def test_tall_tree_kernel_unit_weight_ties(stream):
     """unit weights on a 40 x 40 lattice: most pairs have many shortest paths through several hubs
     (the scan's tie branch); the tall-tree kernel's rows equal the oracle's"""
     side = 40
@@ -113,7 +115,7 @@ def test_tall_tree_kernel_unit_weight_ties():
     idx = g.build_index()
     tc = O.TreeCount(nn, u, v, w)
     srcs = np.arange(0, nn, 37, dtype=np.int32)
-    idx.set_tuning(label_sources=16)
+    idx.set_tuning(label_sources=16, label_stream=stream)
     try:
         d, c, h = idx.rows(srcs)
         bc = idx.bc_sources(srcs)
@@ -317,7 +319,7 @@ def test_200k_tall_tree_rows_and_partial_bc(graph_cache):
     try:
         assert idx.label_group() == 16
         for tune in ({}, {"label_sources": 32}, {"label_warps": 16}, {"label_passes": 2}, {"label_warps": 12},
-                     {"label_sources": 16, "label_warps": 8}):
+                     {"label_sources": 16, "label_warps": 8}, {"label_sources": 16, "label_stream": 1}):
             idx.set_tuning(**tune)
             d, c, h = idx.rows(srcs[:4])
             for k in range(4):
