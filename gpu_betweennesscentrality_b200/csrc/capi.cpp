@@ -1,4 +1,6 @@
 // capi.cpp -- extern "C" boundary of libqbc_b200 (declared in include/qbc_b200.h).
+#include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -143,6 +145,16 @@ int qbc_index_build(const qbc_graph *g, int kind, const int32_t *node_order, int
   });
 }
 
+// Vertices whose min-degree elimination runs on the device (the dense tail, device_dense_eliminate)
+// in a device build: the last 16,384 of graphs with at least 262,144 vertices (1M grid: the last
+// 16,384 eliminations are 2.9 of the host's 5.0 s).  Test hook: QBC_DENSE_TAIL overrides it (0
+// disables the tail; a value >= n eliminates the whole graph on the device).
+static int32_t dense_tail_size(int32_t n) {
+  const char *e = std::getenv("QBC_DENSE_TAIL");
+  if (e && *e) return std::max<int32_t>(0, (int32_t)std::strtol(e, nullptr, 10));
+  return n >= 262144 ? 16384 : 0;
+}
+
 int qbc_index_build_device(const qbc_graph *g, int kind, const int32_t *node_order, int device, qbc_index **out) {
   return guarded([&] {
     need(g && out, "null argument");
@@ -158,8 +170,9 @@ int qbc_index_build_device(const qbc_graph *g, int kind, const int32_t *node_ord
     qbc::Separators seps;
     std::vector<int32_t> o;
     if (node_order) o.assign(node_order, node_order + g->g.n);
+    const qbc::TailEngine tail = [device](qbc::DenseTail &dt) { qbc::device_dense_eliminate(device, dt); };
     p->h.host = qbc::prepare_index(g->g, kind == QBC_INDEX_MHL ? qbc::IndexKind::MHL : qbc::IndexKind::H2H,
-                                   node_order ? &o : nullptr, seps);
+                                   node_order ? &o : nullptr, seps, dense_tail_size(g->g.n), tail);
     qbc::device_build(p->h, device, seps);
     *out = p.release();
   });

@@ -2430,6 +2430,217 @@ void device_set_chunk(Handle &h, int32_t chunk) {
   alloc_scratch(h, d);
 }
 
+// ------------------------------------------------------------------------------- dense elimination
+// The last r vertices of the min-degree elimination (TreeDecomp.cpp:54-208 semantics, as the host's
+// eliminate): near the root the separators are large (hundreds of vertices) and the host spends
+// most of its time there on the k^2 shortcut updates of each step.  Here the remaining graph is a
+// dense r x r matrix of (length, count bits, max hop) entries, absent = kAbsentLen, and each step
+// is two launches: k_dense_pick (one CTA: the live vertex of minimum (degree, id), its row
+// compacted into the separator list in column order) and k_dense_update (one warp per separator
+// vertex u: the shortcuts through x to every other separator vertex, with the host's rule -- a
+// shorter length replaces, an equal one adds the count and keeps the larger hop -- then u's entry
+// for x removed).  The picks, separators and so the tree and rows are the host elimination's: the
+// separator order differs (column order here) and nothing downstream depends on it.
+constexpr int32_t kAbsentLen = 0x7fffffff;
+
+__global__ void k_dense_clear(int4 *M, int64_t count) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+    M[i] = make_int4(kAbsentLen, 0, 0, 0);
+}
+
+__global__ void k_dense_scatter(int4 *M, int32_t r, const int32_t *__restrict__ row, const int4 *__restrict__ ent,
+                                int64_t m) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+    const int4 e = ent[i];
+    M[(int64_t)row[i] * r + e.x] = make_int4(e.y, e.z, e.w, 0);
+  }
+}
+
+constexpr int kPickThreads = 1024;
+
+__global__ void __launch_bounds__(kPickThreads) k_dense_pick(const int4 *__restrict__ M, const int32_t *__restrict__ deg,
+                                                             uint8_t *alive, int32_t r, int32_t step, int32_t *order,
+                                                             int4 *xlist, int32_t *xcount, int4 *sep, int64_t *sep_off) {
+  __shared__ unsigned long long s_best[kPickThreads / 32];
+  __shared__ int32_t s_cnt[kPickThreads / 32];
+  __shared__ int32_t s_x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  unsigned long long best = ~0ull;
+  for (int i = tid; i < r; i += kPickThreads)
+    if (alive[i]) best = min(best, ((unsigned long long)(uint32_t)deg[i] << 32) | (uint32_t)i);
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) best = min(best, __shfl_xor_sync(kFull, best, o));
+  if (lane == 0) s_best[warp] = best;
+  __syncthreads();
+  if (warp == 0) {
+    best = s_best[lane];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) best = min(best, __shfl_xor_sync(kFull, best, o));
+    if (lane == 0) {
+      const int32_t x = (int32_t)(best & 0xffffffffu);
+      s_x = x;
+      alive[x] = 0;
+      order[step] = x;
+    }
+  }
+  __syncthreads();
+  const int32_t x = s_x;
+  // row x compacted in column order: each thread takes a contiguous range of columns
+  const int per = (r + kPickThreads - 1) / kPickThreads;
+  const int c0 = min(r, tid * per), c1 = min(r, c0 + per);
+  const int4 *row = M + (int64_t)x * r;
+  int mine = 0;
+  for (int c = c0; c < c1; c++) mine += row[c].x != kAbsentLen;
+  int incl = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_cnt[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int w = s_cnt[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, w, o);
+      if (lane >= o) w += y;
+    }
+    s_cnt[lane] = w;  // inclusive warp totals
+  }
+  __syncthreads();
+  int p = incl - mine + (warp > 0 ? s_cnt[warp - 1] : 0);
+  const int total = s_cnt[kPickThreads / 32 - 1];
+  const int64_t so = sep_off[step];
+  for (int c = c0; c < c1; c++) {
+    const int4 e = row[c];
+    if (e.x != kAbsentLen) {
+      const int4 v = make_int4(c, e.x, e.y, e.z);
+      xlist[p] = v;
+      sep[so + p] = v;
+      p++;
+    }
+  }
+  if (tid == 0) {
+    *xcount = total;
+    sep_off[step + 1] = so + total;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_dense_update(int4 *M, int32_t *deg, int32_t r, const int4 *__restrict__ xlist,
+                                                      const int32_t *__restrict__ xcount,
+                                                      const int32_t *__restrict__ order, int32_t step) {
+  const int k = *xcount, x = order[step];
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5); i < k; i += warps) {
+    const int4 a = xlist[i];
+    int4 *row = M + (int64_t)a.x * r;
+    int added = 0;
+    for (int j = lane; j < k; j += 32) {
+      if (j == i) continue;
+      const int4 b = xlist[j];
+      const int nl = a.y + b.y;
+      const int nc = (int)((unsigned)a.z * (unsigned)b.z);
+      const int nh = a.w + b.w;
+      const int4 e = row[b.x];
+      if (e.x == kAbsentLen) {
+        row[b.x] = make_int4(nl, nc, nh, 0);
+        added++;
+      } else if (nl < e.x) {
+        row[b.x] = make_int4(nl, nc, nh, 0);
+      } else if (nl == e.x) {
+        row[b.x] = make_int4(e.x, (int)((unsigned)e.y + (unsigned)nc), max(e.z, nh), 0);
+      }
+    }
+    added = __reduce_add_sync(kFull, added);
+    if (lane == 0) {
+      row[x] = make_int4(kAbsentLen, 0, 0, 0);
+      deg[a.x] += added - 1;
+    }
+  }
+}
+
+// device buffers freed on every exit of the function that owns them
+struct DevBufs {
+  std::vector<void *> p;
+  DevBufs() = default;
+  DevBufs(const DevBufs &) = delete;
+  DevBufs &operator=(const DevBufs &) = delete;
+  ~DevBufs() {
+    for (void *q : p) cudaFree(q);
+  }
+  template <class T>
+  T *get(size_t count) {
+    void *q = nullptr;
+    CK(cudaMalloc(&q, std::max<size_t>(1, count) * sizeof(T)));
+    p.push_back(q);
+    return (T *)q;
+  }
+};
+
+void device_dense_eliminate(int device, DenseTail &dt) {
+  NvtxRange range("qbc.dense_eliminate");
+  CK(cudaSetDevice(device));
+  const int32_t r = dt.r;
+  if (r <= 0) {
+    dt.order.clear();
+    dt.x_off.assign(1, 0);
+    dt.x.clear();
+    return;
+  }
+  const int64_t m = dt.off[r];
+  const int64_t cap = std::max<int64_t>(1, (int64_t)r * (r - 1) / 2);  // every pair at most once
+  DevBufs buf;
+  int4 *M = buf.get<int4>((size_t)r * r);
+  int32_t *deg = buf.get<int32_t>(r);
+  uint8_t *alive = buf.get<uint8_t>(r);
+  int32_t *order = buf.get<int32_t>(r);
+  int4 *xlist = buf.get<int4>(r);
+  int32_t *xcount = buf.get<int32_t>(1);
+  int4 *sep = buf.get<int4>((size_t)cap);
+  int64_t *sep_off = buf.get<int64_t>((size_t)r + 1);
+  int32_t *row = buf.get<int32_t>((size_t)m);
+  int4 *ent = buf.get<int4>((size_t)m);
+  std::vector<int32_t> hrow((size_t)m), hdeg((size_t)r);
+  for (int32_t i = 0; i < r; i++) {
+    hdeg[i] = (int32_t)(dt.off[i + 1] - dt.off[i]);
+    for (int64_t e = dt.off[i]; e < dt.off[i + 1]; e++) hrow[e] = i;
+  }
+  cudaStream_t st;
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  } sg{st};
+  CK(cudaMemcpyAsync(row, hrow.data(), (size_t)m * 4, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ent, dt.ent.data(), (size_t)m * 16, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(deg, hdeg.data(), (size_t)r * 4, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(alive, 1, (size_t)r, st));
+  CK(cudaMemsetAsync(sep_off, 0, sizeof(int64_t), st));
+  k_dense_clear<<<148 * 8, 256, 0, st>>>(M, (int64_t)r * r);
+  k_dense_scatter<<<148 * 8, 256, 0, st>>>(M, r, row, ent, m);
+  CK(cudaGetLastError());
+  for (int32_t s = 0; s < r; s++) {
+    k_dense_pick<<<1, kPickThreads, 0, st>>>(M, deg, alive, r, s, order, xlist, xcount, sep, sep_off);
+    k_dense_update<<<148 * 4, 256, 0, st>>>(M, deg, r, xlist, xcount, order, s);
+  }
+  CK(cudaGetLastError());
+  dt.order.resize((size_t)r);
+  dt.x_off.resize((size_t)r + 1);
+  CK(cudaMemcpyAsync(dt.order.data(), order, (size_t)r * 4, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(dt.x_off.data(), sep_off, ((size_t)r + 1) * 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const int64_t total = dt.x_off[r];
+  if (total < 0 || total > cap) throw Error(QBC_ECUDA, "dense elimination: separator total out of range");
+  dt.x.resize((size_t)total * 4);
+  if (total) CK(cudaMemcpyAsync(dt.x.data(), sep, (size_t)total * 16, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+}
+
 // ------------------------------------------------------------------------------- device row fill
 // Label rows built on the device (TreeDecomp.cpp:388-450 semantics, as the host builders): node p's
 // row only reads rows of its separator vertices and ancestors, which sit at smaller depth, so the

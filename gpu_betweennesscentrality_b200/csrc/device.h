@@ -39,6 +39,9 @@ struct Handle {
 };
 
 void device_upload(Handle &h, int device);
+// The last dt.r vertices of a min-degree elimination on the device (a dense matrix, one pick and
+// one shortcut update per step); fills dt.order / dt.x_off / dt.x.
+void device_dense_eliminate(int device, DenseTail &dt);
 // Uploads the index structure and fills its label rows on the device (host rows stay empty).
 void device_build(Handle &h, int device, const Separators &seps);
 // Copies device-built label rows to the host index (no-op when they are there already).

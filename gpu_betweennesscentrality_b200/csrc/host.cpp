@@ -290,7 +290,47 @@ struct MinDegreeHeap {
   }
 };
 
-Elimination eliminate(const Graph &g, const std::vector<int32_t> *fixed_order) {
+// The last tail_r steps handed to `tail` (min-degree elimination only): the vertices still present
+// and their adjacency go out in local ids, the rest of the order and its separators come back.
+static void run_tail(Elimination &el, std::vector<std::vector<Adj>> &adj, int32_t n, int32_t step,
+                     const TailEngine &tail) {
+  DenseTail dt;
+  std::vector<int32_t> loc((size_t)n, -1);
+  for (int32_t v = 0; v < n; v++)
+    if (el.rank[v] < 0) {
+      loc[v] = (int32_t)dt.ids.size();
+      dt.ids.push_back(v);
+    }
+  dt.r = (int32_t)dt.ids.size();
+  dt.off.assign((size_t)dt.r + 1, 0);
+  for (int32_t i = 0; i < dt.r; i++) dt.off[i + 1] = dt.off[i] + (int64_t)adj[dt.ids[i]].size();
+  dt.ent.resize((size_t)dt.off[dt.r] * 4);
+  for (int32_t i = 0; i < dt.r; i++) {
+    int64_t o = dt.off[i] * 4;
+    for (const Adj &a : adj[dt.ids[i]]) {
+      dt.ent[o++] = loc[a.v];
+      dt.ent[o++] = a.len;
+      dt.ent[o++] = (int32_t)a.cnt;
+      dt.ent[o++] = a.hop;
+    }
+  }
+  tail(dt);
+  if ((int32_t)dt.order.size() != dt.r || (int32_t)dt.x_off.size() != dt.r + 1)
+    throw Error(QBC_ECUDA, "dense elimination returned a wrong-sized result");
+  for (int32_t s = 0; s < dt.r; s++) {
+    const int32_t x = dt.ids[dt.order[s]];
+    el.rank[x] = step + s;
+    el.order.push_back(x);
+    const int64_t b = dt.x_off[s], e = dt.x_off[s + 1];
+    el.width = std::max(el.width, (int32_t)(e - b));
+    for (int64_t i = b; i < e; i++)
+      el.x.push_back({dt.ids[dt.x[4 * i]], dt.x[4 * i + 1], (uint32_t)dt.x[4 * i + 2], dt.x[4 * i + 3]});
+    el.x_off.push_back((int64_t)el.x.size());
+  }
+}
+
+Elimination eliminate(const Graph &g, const std::vector<int32_t> *fixed_order, int32_t tail_r = 0,
+                      const TailEngine &tail = {}) {
   const int32_t n = g.n;
   const int nthreads = hardware_threads(0);
   std::vector<std::vector<int32_t>> stamp_t, where_t;  // per-thread stamps for large separators
@@ -315,6 +355,10 @@ Elimination eliminate(const Graph &g, const std::vector<int32_t> *fixed_order) {
   }
   std::vector<Adj> X;
   for (int32_t step = 0; step < n; step++) {
+    if (tail && !fixed_order && tail_r > 0 && n - step == tail_r) {
+      run_tail(el, adj, n, step, tail);
+      break;
+    }
     int32_t x;
     if (fixed_order) {
       x = by_rank[step];
@@ -513,7 +557,8 @@ void fill_ancestor_rows(Index &ix) {
 
 // Elimination (min-degree for MHL, the order file's for H2H) and tree, without label rows; the
 // separator list of each tree node goes to `seps` in tid space for the device row fill.
-Index prepare_index(const Graph &g, IndexKind kind, const std::vector<int32_t> *node_order, Separators &seps) {
+Index prepare_index(const Graph &g, IndexKind kind, const std::vector<int32_t> *node_order, Separators &seps,
+                    int32_t tail_r, const TailEngine &tail) {
   if (kind == IndexKind::H2H) {
     if (!node_order || (int32_t)node_order->size() != g.n) throw Error(QBC_EINVAL, "order has wrong length");
     std::vector<char> seen((size_t)g.n, 0);
@@ -523,7 +568,7 @@ Index prepare_index(const Graph &g, IndexKind kind, const std::vector<int32_t> *
       seen[o] = 1;
     }
   }
-  Elimination el = eliminate(g, kind == IndexKind::H2H ? node_order : nullptr);
+  Elimination el = eliminate(g, kind == IndexKind::H2H ? node_order : nullptr, std::min(tail_r, g.n), tail);
   Index ix;
   ix.kind = kind;
   make_tree(g, el, ix, false);

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -68,8 +69,26 @@ struct Separators {
   std::vector<int64_t> off;
   std::vector<int32_t> ent;
 };
+// The last r vertices of a min-degree elimination, handed to another engine (the device's dense
+// elimination, device_dense_eliminate): the vertices still present, ascending (local id = index),
+// with their current adjacency in local ids.  The engine returns the rest of the elimination: the
+// local ids in elimination order (minimum current degree, smaller id first, as the host) and each
+// step's separator, (local column, shortcut length, path count bits, max hop) per entry.
+struct DenseTail {
+  int32_t r = 0;
+  std::vector<int32_t> ids;  // global vertex ids, ascending
+  std::vector<int64_t> off;  // r + 1: vertex i's entries are ent[4*off[i] .. 4*off[i+1])
+  std::vector<int32_t> ent;  // (local column, length, count bits, max hop)
+  std::vector<int32_t> order;  // result: local ids in elimination order
+  std::vector<int64_t> x_off;  // result: r + 1
+  std::vector<int32_t> x;      // result: separator entries as in `ent`
+};
+using TailEngine = std::function<void(DenseTail &)>;
+
 // Elimination and tree only (no label rows: dis/ch/anc/aend stay empty); max_label is unknown (0).
-Index prepare_index(const Graph &g, IndexKind kind, const std::vector<int32_t> *node_order, Separators &seps);
+// With `tail` (min-degree elimination only), the last `tail_r` vertices are eliminated by it.
+Index prepare_index(const Graph &g, IndexKind kind, const std::vector<int32_t> *node_order, Separators &seps,
+                    int32_t tail_r = 0, const TailEngine &tail = {});
 
 // Per-entry ancestor ids (anc) and their subtree ends (aend) of every row, from the tree links
 // (a row is its parent's row plus the node itself).

@@ -97,3 +97,40 @@ def test_known_graphs_device_build(name):
     bc = dev.bc_all()
     _same_rows(host, dev)
     assert np.allclose(bc, expect, rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("tail", [64, 700, 100000])
+def test_mhl_rows_dense_tail_2k(monkeypatch, tail):
+    """the last `tail` vertices of the min-degree elimination eliminated on the device as a dense
+    matrix (all of them for 100000): same picks, separators, tree and rows as the host"""
+    monkeypatch.setenv("QBC_DENSE_TAIL", str(tail))
+    n, u, v, w = synth.read_graph_lines(os.path.join(GOLDEN, "g2k.txt"))
+    host, dev = _pair(n, u, v, w)
+    bc = dev.bc_all()
+    _same_rows(host, dev)
+    assert rel_err(bc, O.TreeCount(n, u, v, w).bc(O.Arcs(n, u, v, w))) <= BC_RTOL
+
+
+@pytest.mark.parametrize("n_target,seed,sc,tail", [(3000, 6, 0.02, 3000), (20000, 3, 0.0, 2500)])
+def test_mhl_rows_dense_tail_generated(monkeypatch, n_target, seed, sc, tail):
+    """shortcut vertices (more than four arcs, long shortcuts) and a 20k grid with a 2,500-vertex
+    dense tail: rows bit-identical to the host build"""
+    monkeypatch.setenv("QBC_DENSE_TAIL", str(tail))
+    n, u, v, w = grid_lines(n_target, seed=seed, shortcut_frac=sc)
+    host, dev = _pair(n, u, v, w)
+    _same_rows(host, dev)
+
+
+def test_mhl_rows_dense_tail_200k(monkeypatch, graph_cache):
+    """200k grid: the default device build (host elimination) and one with a 16,384-vertex dense
+    tail on the device give identical trees and rows"""
+    path = synth.cached_graph(graph_cache, 200000, seed=1)
+    g = Q.Graph(device=0)
+    g.ReadGraph(path)
+    monkeypatch.setenv("QBC_DENSE_TAIL", "0")
+    a = g.build_index(on_device=True).export()
+    monkeypatch.setenv("QBC_DENSE_TAIL", "16384")
+    b = g.build_index(on_device=True).export()
+    for f in FIELDS:
+        assert np.array_equal(a[f], b[f]), f
+    assert np.array_equal(a["ch"], b["ch"])
