@@ -431,6 +431,48 @@ def config_shortcuts_1m(q, args, dev, flush, peak, peak_src):
     return out
 
 
+def config_mhl_1m(q, args, dev, flush, peak, peak_src):
+    """The label path on a tree too tall for the 32-source label kernel: MHL-QBC partial BC on the
+    1,000,000-vertex grid without shortcuts (tree height 2,725), rows filled on the device (its
+    last 16,384 eliminations too), default tuning: the 16-source tall-tree label kernel."""
+    import torch
+    from gpu_betweennesscentrality_b200 import synth
+
+    t = time.perf_counter()
+    g = synth.grid_graph(args.shortcut_n, seed=args.seed)
+    u, v, w = g.arcs()
+    t_gen = time.perf_counter() - t
+    G = q.Graph(device=0)
+    G.ReadLines(g.n, u, v, w)
+    t = time.perf_counter()
+    idx = G.build_index(on_device=True)
+    torch.cuda.synchronize()
+    t_build = time.perf_counter() - t
+    info = idx.info()
+    n = g.n
+    sample = np.sort(np.random.default_rng(args.seed + 1).choice(n, min(n, 4096), replace=False)).astype(np.int32)
+    steps = min(args.steps, 3)
+    clocks = ClockSampler(dev.index or 0).start()
+    ms, stats, _ = device_sweep(idx, sample, steps, 3, dev, flush)
+    clk = clocks.stop()
+    value = len(sample) * steps / (sum(ms) / 1e3)
+    e2e, _ = e2e_rate(idx, sample, 1)
+    roof = label_roofline(idx, sample, n, stats, steps, peak, peak_src, clk.get("sm_mhz") or 1965.0)
+    out = {"workload": f"MHL-QBC partial BC over a seeded sample of {len(sample)} sources, seeded perturbed grid "
+                       f"n={n} without shortcuts (tree height {int(info[3])}: the tall-tree label kernel)",
+           "n": n, "sources_per_step": int(len(sample)), "steps": steps, "warmup": 3,
+           "value": value, "unit": "sources/s", "ms_per_step": sum(ms) / steps,
+           "e2e": {"value": e2e, "unit": "sources/s", "h2d_bytes_per_step": int(4 * len(sample)),
+                   "d2h_bytes_per_step": int(8 * n)},
+           "index": {"tree_height": int(info[3]), "tree_width": int(info[4]), "label_entries": int(info[2]),
+                     "device_bytes": int(info[5]), "generate_s": round(t_gen, 2),
+                     "build_s": round(t_build, 3), "build": "device rows and dense elimination tail"},
+           "tuning": idx.get_tuning(), "roofline": roof, "clocks": clk, "gpu_launches": int(stats["launches"])}
+    del idx, G
+    gc.collect()
+    return out
+
+
 def config_rq_200k(q, args, dev, flush):
     """RQ on the 200,000-vertex grid + 2 % shortcuts with a uniform query set of 4,096 vertices."""
     from gpu_betweennesscentrality_b200 import synth
@@ -639,6 +681,7 @@ def main():
             extra["qbc_2k"] = config_qbc_2k(q, args)
             extra["rq_200k"] = config_rq_200k(q, args, dev, flush)
             extra["shortcuts_1m"] = config_shortcuts_1m(q, args, dev, flush, peak, peak_src)
+            extra["mhl_1m"] = config_mhl_1m(q, args, dev, flush, peak, peak_src)
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "sources/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
