@@ -274,7 +274,7 @@ def plain_rate(idx, sources, k):
 # ------------------------------------------------------------------------------- rooflines
 def label_roofline(idx, shard, n, stats, steps, peak, peak_src, sm_mhz):
     """Dominant kernel of the label path: the packed label scan.  DRAM model per launch: target rows
-    copied once per CTA group of sources (32; 16 for the tall-tree form), each up to the group's
+    copied once per CTA group of sources (32; 16 for the lane-pair forms), each up to the group's
     deepest LCA depth (4 B per entry, exact from the index), plus the (dist, count, rho) records
     and hop layers written (20 B per pair); cross-checked against ncu in
     profiles/k_label_scan_packed_50k.md (model 9.12 GB, ncu 9.80 GB per 4,096-source launch).  The algorithmic figure of the workload's byte model (12 B
@@ -296,7 +296,7 @@ def label_roofline(idx, shard, n, stats, steps, peak, peak_src, sm_mhz):
     smem_roof = 32.0 if tall else 256.0 / 12.0
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "peak_source": peak_src,
-            "kernel": "k_label_scan_tall" if tall else "k_label_scan_packed", "sources_per_cta": per_cta,
+            "kernel": idx.label_kernel(), "sources_per_cta": per_cta,
             "dram_model_bytes_per_launch": dram_step / launches_step, "launch_ms": launch_ms,
             "launches_per_step": launches_step, "label_ms_per_step": label_ms_step,
             "dependency_ms_per_step": stats["dep_ms"] / steps,
@@ -306,7 +306,7 @@ def label_roofline(idx, shard, n, stats, steps, peak, peak_src, sm_mhz):
                              "frac": ent_per_clk / smem_roof, "issue_peak": 128.0 / 3.5,
                              "note": "shared-memory roof: a 16-byte shared load takes at least one wavefront "
                                      "per half-warp (2 for a full-warp broadcast, measured); " +
-                                     ("tall-tree form: lane pairs share a source row, so 8 wavefronts per 8 "
+                                     ("16-source forms (rows16, tall): lane pairs share a source row, so 8 wavefronts per 8 "
                                       "entries of 32 pairs (32.0)" if tall else
                                       "32 distinct source rows + broadcast target: 12 wavefronts per 8 entries "
                                       "of 32 pairs (21.3)") +

@@ -164,6 +164,12 @@ class Index:
         check(lib().qbc_index_label_group(self.h, ptr(g, i32p)))
         return int(g[0])
 
+    def label_kernel(self) -> str:
+        """Name of the kernel the batched per-source rows come from under the current tuning."""
+        buf = C.create_string_buffer(64)
+        check(lib().qbc_index_label_kernel(self.h, buf, 64))
+        return buf.value.decode()
+
     TUNING_KEYS = ("lanes_per_source", "label_threads", "split", "chunk", "dep_threads", "dep_form", "queue_depth",
                    "label_warps", "label_tile", "label_passes", "sweep_delta", "sweep_threads", "label_sources",
                    "label_stream")

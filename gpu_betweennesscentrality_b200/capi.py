@@ -45,6 +45,7 @@ SIGNATURES = {
     "qbc_index_scan_entries": (C.c_int, [vp, i32p, C.c_int32, i64p]),
     "qbc_index_group_entries": (C.c_int, [vp, i32p, C.c_int32, C.c_int32, i64p]),
     "qbc_index_label_group": (C.c_int, [vp, i32p]),
+    "qbc_index_label_kernel": (C.c_int, [vp, C.c_char_p, C.c_int32]),
     "qbc_index_free": (None, [vp]),
     "qbc_index_export": (C.c_int, [vp, i32p, i32p, i32p, i64p, i32p, i32p, i32p]),
     "qbc_index_set_tuning": (C.c_int, [vp, i32p, C.c_int32]),

@@ -255,6 +255,15 @@ int qbc_index_label_group(qbc_index *idx, int32_t *sources_per_cta) {
   });
 }
 
+int qbc_index_label_kernel(qbc_index *idx, char *name, int32_t cap) {
+  return guarded([&] {
+    need(idx && name && cap > 0, "null argument or cap < 1");
+    const char *k = qbc::device_label_kernel(idx->h);
+    std::strncpy(name, k, (size_t)cap - 1);
+    name[cap - 1] = '\0';
+  });
+}
+
 void qbc_index_free(qbc_index *idx) { delete idx; }
 
 int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int32_t *send, int64_t *lab_off,
@@ -299,7 +308,8 @@ int qbc_index_set_tuning(qbc_index *idx, const int32_t *params, int32_t nparams)
     if (nparams > 9) need(params[9] >= 0 && params[9] <= 2, "label passes must be 0, 1 or 2");
     if (nparams > 10) need(params[10] >= 0, "sweep bucket width must be >= 0");
     if (nparams > 11)
-      need(params[11] == 0 || params[11] == 256 || params[11] == 512 || params[11] == 1024, "sweep threads must be 0, 256, 512 or 1024");
+      need(params[11] == 0 || params[11] == 256 || params[11] == 512 || params[11] == 1024 || params[11] == 2048,
+           "sweep threads must be 0, 256, 512, 1024 or 2048 (four 512-thread CTAs per SM)");
     if (nparams > 12) need(params[12] == 0 || params[12] == 16 || params[12] == 32, "label sources must be 0, 16 or 32");
     if (nparams > 13) need(params[13] >= 0 && params[13] <= 2, "label stream must be 0, 1 or 2");
     for (int32_t i = 0; i < nparams && i < kTuningFields; i++) *f[i] = params[i];

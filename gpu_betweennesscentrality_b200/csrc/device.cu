@@ -23,13 +23,17 @@
 // measured ~2x slower in total).
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <climits>
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "device_state.h"
@@ -1756,43 +1760,59 @@ __global__ void __launch_bounds__(256, 3) k_dependency_warp(DepArgs a, const int
 // reads layer L as [cnt[L - 1], cnt[L]) through the pointer cnt - 1.
 constexpr int kDepLayerCap = 2046;
 
-template <bool MASK, class CNT>
+// The label-free sweep leaves its Kahn queue as the level queue (PRE): wave L is hop layer L, kept
+// at [ws[L], ws[L + 1]) of the order row with the starts ws in the second half of the slot's
+// layer-counter row, so the layer sort below is skipped; cnt[i] = ws[i + 1] is the same array the
+// sort would leave (layer L at [cnt[L - 1], cnt[L]), the source alone in layer 0 at the front).
+__device__ __forceinline__ const int32_t *sweep_wave_starts(const DepArgs &a, int slot) {
+  return a.lcnt + (size_t)slot * 2 * (a.n_pad + 2) + (a.n_pad + 2);
+}
+
+template <bool MASK, bool PRE, class CNT>
 __device__ __forceinline__ void dep_cta_pipe_body(const DepArgs &a, int slot, int maxL, CNT *cnt, int *red) {
   const int s = a.src[slot];
   const size_t base = (size_t)slot * a.n_pad;
   const RowView<int4> rec{a.rec, slot, a.ns};
   const RowView<const int32_t> hop{a.hop, slot, a.ns};
   int32_t *order = a.order + base;
-  for (int i = threadIdx.x; i <= maxL + 1; i += blockDim.x) cnt[i] = 0;
-  __syncthreads();
-  // layer histogram, then the counting sort of the source's vertices by layer; each thread has
-  // kHopBatch hop loads in flight before its atomics
   const int W = blockDim.x, tid = threadIdx.x;
-  for (int v0 = 0; v0 < a.n; v0 += W * kHopBatch) {
-    int hv[kHopBatch];
-#pragma unroll
-    for (int q = 0; q < kHopBatch; q++) {
-      const int v = v0 + q * W + tid;
-      hv[q] = (v < a.n && v != s) ? hop[v] : -1;
+  if constexpr (PRE) {
+    if constexpr (!std::is_const<CNT>::value) {  // shared counters: copy the starts in
+      const int32_t *ws = sweep_wave_starts(a, slot);
+      for (int i = tid; i <= maxL; i += W) cnt[i] = __ldcg(ws + i + 1);
     }
+    __syncthreads();
+  } else {
+    for (int i = threadIdx.x; i <= maxL + 1; i += blockDim.x) cnt[i] = 0;
+    __syncthreads();
+    // layer histogram, then the counting sort of the source's vertices by layer; each thread has
+    // kHopBatch hop loads in flight before its atomics
+    for (int v0 = 0; v0 < a.n; v0 += W * kHopBatch) {
+      int hv[kHopBatch];
 #pragma unroll
-    for (int q = 0; q < kHopBatch; q++)
-      if (hv[q] >= 0) layer_slot(cnt, hv[q]);
-  }
-  __syncthreads();
-  block_exclusive_scan(cnt, maxL + 1, red);
-  for (int v0 = 0; v0 < a.n; v0 += W * kHopBatch) {
-    int hv[kHopBatch];
+      for (int q = 0; q < kHopBatch; q++) {
+        const int v = v0 + q * W + tid;
+        hv[q] = (v < a.n && v != s) ? hop[v] : -1;
+      }
 #pragma unroll
-    for (int q = 0; q < kHopBatch; q++) {
-      const int v = v0 + q * W + tid;
-      hv[q] = (v < a.n && v != s) ? hop[v] : -1;
+      for (int q = 0; q < kHopBatch; q++)
+        if (hv[q] >= 0) layer_slot(cnt, hv[q]);
     }
+    __syncthreads();
+    block_exclusive_scan(cnt, maxL + 1, red);
+    for (int v0 = 0; v0 < a.n; v0 += W * kHopBatch) {
+      int hv[kHopBatch];
 #pragma unroll
-    for (int q = 0; q < kHopBatch; q++)
-      if (hv[q] >= 0) order[layer_slot(cnt, hv[q])] = v0 + q * W + tid;
+      for (int q = 0; q < kHopBatch; q++) {
+        const int v = v0 + q * W + tid;
+        hv[q] = (v < a.n && v != s) ? hop[v] : -1;
+      }
+#pragma unroll
+      for (int q = 0; q < kHopBatch; q++)
+        if (hv[q] >= 0) order[layer_slot(cnt, hv[q])] = v0 + q * W + tid;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   const CNT *start = cnt - 1;  // layer L is [start[L], start[L + 1]) for L >= 1
   // Pipeline over steps: the queue entry of a step is loaded three steps before it is computed,
   // its own record two, its arcs one; a step then waits only for its successors' records (rho
@@ -1850,8 +1870,9 @@ __device__ __forceinline__ void dep_cta_pipe_body(const DepArgs &a, int slot, in
 }
 
 // The body is instantiated for shared counters (the usual case: shared-memory atomics and loads)
-// and for the per-slot global counters of DAGs deeper than kDepLayerCap layers; MASK for records
-// that carry DAG-successor masks (the label-free sweep's), so the label path's code has no mask test.
+// and for the per-slot global counters of DAGs deeper than kDepLayerCap layers; MASK (with PRE) for
+// the label-free sweep's rows, whose records carry DAG-successor masks and whose queue is sorted by
+// layer already, so the label path's code has neither the mask test nor the wave starts.
 template <bool MASK>
 __global__ void __launch_bounds__(256, 3) k_dependency_cta_pipe(DepArgs a, const int32_t *__restrict__ maxhop) {
   if (rows_failed(a)) return;
@@ -1861,9 +1882,11 @@ __global__ void __launch_bounds__(256, 3) k_dependency_cta_pipe(DepArgs a, const
   if (slot >= a.ns) return;
   const int maxL = maxhop[slot];
   if (maxL <= kDepLayerCap)
-    dep_cta_pipe_body<MASK>(a, slot, maxL, sh_cnt, red);
+    dep_cta_pipe_body<MASK, MASK>(a, slot, maxL, sh_cnt, red);
+  else if constexpr (MASK)  // the sweep's wave starts, read in place
+    dep_cta_pipe_body<true, true>(a, slot, maxL, sweep_wave_starts(a, slot) + 1, red);
   else
-    dep_cta_pipe_body<MASK>(a, slot, maxL, a.lcnt + (size_t)slot * 2 * (a.n_pad + 2), red);
+    dep_cta_pipe_body<false, false>(a, slot, maxL, a.lcnt + (size_t)slot * 2 * (a.n_pad + 2), red);
 }
 
 // QBC: sigma by Kahn waves on the SP-DAG from H2H distances (QBC.cu:335-344, :485-555), then
@@ -2078,16 +2101,33 @@ static int packed_warps(const Handle &h, const DeviceState *d) {
   return packed_stride(h, d, 16) >= d->hmax_pad ? 16 : 8;
 }
 
+// Target tiles per source group (the label kernels' grid is tiles x groups, one CTA per SM): at
+// least four CTAs per SM in all, tiles of at least 8 targets per warp, and among up to twice that
+// many tiles the count whose last wave of CTAs is fullest.  A launch of few groups (a 1M-vertex
+// chunk holds ~40 groups of 16 sources) otherwise ends in a wave that leaves most SMs idle.
+static int label_split(int groups, int warps, int n_pad, int tuned) {
+  if (tuned > 0) return tuned;
+  const int cap = std::max(1, (n_pad / 8) / warps);
+  const int lo = std::min(cap, std::max(1, (148 * 4 + groups - 1) / groups));
+  int best = lo;
+  double best_fill = 0.0;
+  for (int s = lo; s <= std::min(cap, 2 * lo); s++) {
+    const long long ctas = (long long)groups * s;
+    const double fill = (double)ctas / (double)(((ctas + 147) / 148) * 148);
+    if (fill > best_fill + 1e-9) {
+      best_fill = fill;
+      best = s;
+    }
+  }
+  return best;
+}
+
 template <bool C, int W>
 static void launch_label_packed_w(const Handle &h, const DeviceState *d, LabelArgs a, int32_t ns, cudaStream_t st) {
   const int S = packed_stride(h, d, W);
   const size_t smem = packed_smem(W, S);
   const int groups = (ns + 31) / 32;
-  int split = h.tuning.split;
-  if (split <= 0) {
-    split = std::max(1, (148 * 4 + groups - 1) / groups);
-    split = std::min(split, std::max(1, (d->n_pad / 8) / W));
-  }
+  const int split = label_split(groups, W, d->n_pad, h.tuning.split);
   a.stride = S;
   a.split = split;
   dim3 grid(split, groups);
@@ -2110,11 +2150,7 @@ static void launch_label_pair(const Handle &h, const DeviceState *d, LabelArgs a
   const int S = packed_stride(h, d, 12);
   const size_t smem = pair_smem(S);
   const int groups = (ns + 31) / 32;
-  int split = h.tuning.split;
-  if (split <= 0) {
-    split = std::max(1, (148 * 4 + groups - 1) / groups);
-    split = std::min(split, std::max(1, (d->n_pad / 8) / kPairWarps));
-  }
+  const int split = label_split(groups, kPairWarps, d->n_pad, h.tuning.split);
   a.stride = S;
   a.split = split;
   a.multipass = 0;
@@ -2171,8 +2207,7 @@ static void launch_label_tall(const DeviceState *d, LabelArgs a, int32_t ns, cud
   const int S = tall_stride(d);
   const size_t smem = tall_smem(W, R, S);
   const int groups = (ns + kTallSources - 1) / kTallSources;
-  int split = std::max(1, (148 * 4 + groups - 1) / groups);
-  split = std::min(split, std::max(1, (d->n_pad / 8) / W));
+  const int split = label_split(groups, W, d->n_pad, 0);
   a.stride = S;
   a.split = split;
   CK(cudaFuncSetAttribute(k_label_scan_tall<C, W, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -2186,8 +2221,7 @@ static void launch_label_rows16(const DeviceState *d, LabelArgs a, int32_t ns, c
   const int S = tall_stride(d), R = rows16_words(d);
   const size_t smem = rows16_smem(W, S, R);
   const int groups = (ns + kTallSources - 1) / kTallSources;
-  int split = std::max(1, (148 * 4 + groups - 1) / groups);
-  split = std::min(split, std::max(1, (d->n_pad / 8) / W));
+  const int split = label_split(groups, W, d->n_pad, 0);
   a.stride = S;
   a.row_words = R;
   a.split = split;
@@ -2940,7 +2974,13 @@ void device_build(Handle &h, int device, const Separators &seps) {
   NvtxRange nvtx("qbc.build_device");
   Index &ix = h.host;
   try {
-    DeviceState *d = new_state(h, device);
+    DeviceState *d = nullptr;
+    {
+      TraceScope t("device state and arc upload");
+      d = new_state(h, device);
+      CK(cudaStreamSynchronize(d->s_label));
+    }
+    auto t_fill = std::make_unique<TraceScope>("row buffers and device row fill");
     cudaStream_t st = d->s_label;
     const int64_t L = ix.lab_off[ix.n];
     d->dis = dmalloc<int32_t>(d, (size_t)L);
@@ -3037,7 +3077,10 @@ void device_build(Handle &h, int device, const Separators &seps) {
     ix.ch.clear();
     ix.anc.clear();
     ix.aend.clear();
+    t_fill.reset();
+    TraceScope t_fin("per-source scratch");
     finish_state(h, d);
+    if (TraceScope::enabled()) CK(cudaDeviceSynchronize());
   } catch (...) {
     device_release(h);
     throw;
@@ -3069,7 +3112,8 @@ void device_release(Handle &h) {
   cudaSetDevice(d->device);
   cudaDeviceSynchronize();
   void *ptrs[] = {d->depth, d->send, d->arc_off, d->arc_head, d->arc_w, d->arc_rng, d->arc_hw, d->arc4, d->vid_of, d->tid_of, d->parent,
-                  d->lab_off, d->dis, d->ch, d->bc_tid, d->bc_vid, d->err, d->grid_ctl, d->sources};  // dis_sh aliases dis
+                  d->lab_off, d->dis, d->ch, d->bc_tid, d->bc_vid, d->err, d->grid_ctl, d->sources,
+                  d->dsrc_tid, d->dsrc_sorted, d->dsrc_tmp};  // dis_sh aliases dis
   for (void *p : ptrs)
     if (p) cudaFree(p);
   free_scratch(d);
@@ -3112,6 +3156,41 @@ void check_err(DeviceState *d) {
 // ------------------------------------------------------------------------------- drivers
 // Sorts nothing on the device: chunks take the source list in the given order; sources listed in
 // increasing tid order group nearby tree nodes into one CTA.
+// A device source list as tids in tree order, on stream st: the label kernels give consecutive
+// sources to one CTA, and sources of one subtree share most of their ancestors, so a CTA's scans
+// end at similar depths and its target rows are fetched to similar depths (1M grid, 4,096 random
+// sources, tall-tree kernel: 1,874 ms per step in tid order against 2,593 ms in vid order).  The
+// host entry points sort on the host; here the tids are sorted on the device (a radix sort of ns
+// keys over the bits of n - 1).  Buffers grow on demand and stay with the index.
+static const int32_t *device_sources_tid_order(DeviceState *d, const int32_t *d_sources0, int32_t ns, cudaStream_t st) {
+  int bits = 1;
+  while (bits < 31 && ((d->n - 1) >> bits) != 0) bits++;
+  size_t tmp = 0;
+  CK(cub::DeviceRadixSort::SortKeys(nullptr, tmp, (const int32_t *)nullptr, (int32_t *)nullptr, ns, 0, bits, st));
+  if (ns > d->dsrc_cap || tmp > d->dsrc_tmp_bytes) {
+    CK(cudaStreamSynchronize(st));
+    for (void *p : {(void *)d->dsrc_tid, (void *)d->dsrc_sorted, d->dsrc_tmp})
+      if (p) cudaFree(p);
+    d->bytes -= (int64_t)d->dsrc_cap * 8 + (int64_t)d->dsrc_tmp_bytes;
+    d->dsrc_tid = d->dsrc_sorted = nullptr;
+    d->dsrc_tmp = nullptr;
+    d->dsrc_cap = 0;
+    d->dsrc_tmp_bytes = 0;
+    const int32_t cap = std::max(ns, d->dsrc_cap);
+    d->dsrc_tid = dmalloc<int32_t>(d, (size_t)cap);
+    d->dsrc_sorted = dmalloc<int32_t>(d, (size_t)cap);
+    d->dsrc_tmp = dmalloc<unsigned char>(d, tmp);
+    d->dsrc_cap = cap;
+    d->dsrc_tmp_bytes = std::max<size_t>(1, tmp);
+  }
+  k_vid_to_tid<<<(ns + 255) / 256, 256, 0, st>>>(d_sources0, d->tid_of, d->dsrc_tid, ns, d->n, d->err);
+  CK(cudaGetLastError());
+  d->launches++;
+  size_t have = d->dsrc_tmp_bytes;
+  CK(cub::DeviceRadixSort::SortKeys(d->dsrc_tmp, have, d->dsrc_tid, d->dsrc_sorted, ns, 0, bits, st));
+  return d->dsrc_sorted;
+}
+
 void device_bc_sources(Handle &h, const int32_t *d_sources0, int32_t ns, double *d_bc_vid, void *stream) {
   NvtxRange nvtx("qbc.bc_sources_device");
   DeviceState *d = need_dev(h);
@@ -3122,16 +3201,14 @@ void device_bc_sources(Handle &h, const int32_t *d_sources0, int32_t ns, double 
   CK(cudaMemsetAsync(d->bc_tid, 0, (size_t)d->n * 8, d->s_label));
   CK(cudaEventRecord(d->ev_label[1], d->s_label));
   CK(cudaStreamWaitEvent(d->s_dep, d->ev_label[1], 0));
+  const int32_t *tids = ns > 0 ? device_sources_tid_order(d, d_sources0, ns, d->s_label) : nullptr;
   for (int32_t off = 0; off < ns; off += d->chunk) {
     const int b = 0;  // stream order frees the buffer for the next chunk
     const int32_t cnt = std::min(d->chunk, ns - off);
-    k_vid_to_tid<<<(cnt + 255) / 256, 256, 0, d->s_label>>>(d_sources0 + off, d->tid_of, d->src[b], cnt, d->n, d->err);
-    CK(cudaGetLastError());
-    d->launches++;
-    launch_label(h, d, b, d->src[b], cnt, false, d->s_label);
+    launch_label(h, d, b, tids + off, cnt, false, d->s_label);
     // The dependency pass runs right after the scan on the same stream: run concurrently on a
     // second stream the two kernels thrash each other's caches and both slow down ~2x.
-    launch_dep(h, d, b, d->src[b], cnt, d->s_label);
+    launch_dep(h, d, b, tids + off, cnt, d->s_label);
   }
   CK(cudaEventRecord(d->ev_dep[0], d->s_label));
   CK(cudaStreamWaitEvent(user, d->ev_dep[0], 0));
@@ -3174,6 +3251,15 @@ int32_t device_label_group(Handle &h) {
   if (h.host.kind == IndexKind::CSR) return 0;
   if (use_packed(h, d, false)) return tall_warps(h, d) ? kTallSources : 32;
   return plan_label(h, d, std::max(1, d->chunk), false).G;
+}
+
+const char *device_label_kernel(Handle &h) {
+  DeviceState *d = need_dev(h);
+  if (h.host.kind == IndexKind::CSR) return "k_sweep_rows";
+  if (!use_packed(h, d, false)) return "k_label_scan";
+  const TallCfg tc = tall_cfg(h, d);
+  if (tc.warps) return tc.whole ? "k_label_scan_rows16" : "k_label_scan_tall";
+  return packed_warps(h, d) == 12 ? "k_label_scan_pair" : "k_label_scan_packed";
 }
 
 static int32_t *stage_sources(DeviceState *d, const int32_t *sources0, int32_t ns, int32_t n) {

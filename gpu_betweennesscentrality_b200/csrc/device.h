@@ -21,7 +21,8 @@ struct Tuning {
   int32_t label_tile = 0;        // label entries per row staged in shared memory; 0 = all that fit
   int32_t label_passes = 0;      // rows longer than the tile: 0/1 one pass + global tail, 2 several tile passes
   int32_t sweep_delta = 0;       // CSR index: distance bucket width of the shortest-path sweep; 0 = auto
-  int32_t sweep_threads = 0;     // CSR index: threads per CTA of the sweep (256, 512 or 1024; 0 = 512)
+  int32_t sweep_threads = 0;     // CSR index: threads per CTA of the sweep (256, 512 or 1024; 0 = 512);
+                                 // 2048: 512-thread CTAs, four per SM (32 registers a thread)
   int32_t label_sources = 0;     // packed-key label kernel: sources per CTA (32, or 16 with whole rows of
                                  // tall trees in shared memory); 0 = auto
   int32_t label_stream = 0;      // 16-source kernel: 1 whole target rows double-buffered, 2 64-entry
@@ -66,6 +67,8 @@ void device_profiling(Handle &h, bool on);
 void device_stats(Handle &h, double *out);
 // sources per CTA of the batched label scan under the current tuning (0: label-free index)
 int32_t device_label_group(Handle &h);
+// name of the kernel the batched rows come from under the current tuning
+const char *device_label_kernel(Handle &h);
 // rows of each listed source in vid order (cnt/hop may be null)
 void host_rows(Handle &h, const int32_t *sources0, int32_t ns, int32_t *dist, uint32_t *cnt, int32_t *hop);
 

@@ -90,6 +90,12 @@ struct DeviceState {
   double *bc_vid = nullptr;
   int32_t *sources = nullptr;  // staging for host source lists
   int32_t sources_cap = 0;
+  // device source lists (qbc_bc_sources_device): tids, then the same sorted, and the sort's
+  // temporary storage; grown on demand
+  int32_t *dsrc_tid = nullptr, *dsrc_sorted = nullptr;
+  void *dsrc_tmp = nullptr;
+  size_t dsrc_tmp_bytes = 0;
+  int32_t dsrc_cap = 0;
   int32_t *err = nullptr;
   int32_t *grid_ctl = nullptr;  // control block of the cooperative plain sweep (kGridCtlBytes)
   int64_t bytes = 0, scratch_bytes = 0;

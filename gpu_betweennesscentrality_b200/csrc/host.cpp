@@ -314,7 +314,10 @@ static void run_tail(Elimination &el, std::vector<std::vector<Adj>> &adj, int32_
       dt.ent[o++] = a.hop;
     }
   }
-  tail(dt);
+  {
+    TraceScope t("dense elimination tail");
+    tail(dt);
+  }
   if ((int32_t)dt.order.size() != dt.r || (int32_t)dt.x_off.size() != dt.r + 1)
     throw Error(QBC_ECUDA, "dense elimination returned a wrong-sized result");
   for (int32_t s = 0; s < dt.r; s++) {
@@ -568,9 +571,14 @@ Index prepare_index(const Graph &g, IndexKind kind, const std::vector<int32_t> *
       seen[o] = 1;
     }
   }
-  Elimination el = eliminate(g, kind == IndexKind::H2H ? node_order : nullptr, std::min(tail_r, g.n), tail);
+  Elimination el;
+  {
+    TraceScope t("elimination");
+    el = eliminate(g, kind == IndexKind::H2H ? node_order : nullptr, std::min(tail_r, g.n), tail);
+  }
   Index ix;
   ix.kind = kind;
+  TraceScope t("tree and separators");
   make_tree(g, el, ix, false);
   const int32_t n = g.n;
   std::vector<int64_t> xs((size_t)n, 0);

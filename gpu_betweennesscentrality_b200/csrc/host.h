@@ -1,13 +1,45 @@
 // host.h -- host-side types of libqbc_b200: graph, tree-decomposition index, errors.
 #pragma once
 
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 namespace qbc {
+
+// Wall-clock time of a scope on stderr ("qbc: <name> <ms> ms") when the environment variable
+// QBC_TRACE is set and not "0": the phases of an index build (elimination, dense tail, tree, row
+// fill, scratch) for a user sizing a deployment.  Phases that enqueue device work end with a
+// synchronisation, so their times include it.
+struct TraceScope {
+  explicit TraceScope(const char *name) : name_(name) {
+    if (enabled()) t0_ = std::chrono::steady_clock::now(), on_ = true;
+  }
+  ~TraceScope() {
+    if (on_)
+      std::fprintf(stderr, "qbc: %s %.1f ms\n", name_,
+                   std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count());
+  }
+  TraceScope(const TraceScope &) = delete;
+  TraceScope &operator=(const TraceScope &) = delete;
+  static bool enabled() {
+    static const bool on = [] {
+      const char *e = std::getenv("QBC_TRACE");
+      return e && *e && std::string(e) != "0";
+    }();
+    return on;
+  }
+
+ private:
+  const char *name_;
+  std::chrono::steady_clock::time_point t0_{};
+  bool on_ = false;
+};
 
 constexpr int32_t kInf = 999999999;  // TreeDecomp INF (src/TreeCount/TreeDecomp.h:58)
 

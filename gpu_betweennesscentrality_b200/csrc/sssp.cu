@@ -183,8 +183,10 @@ __device__ __forceinline__ Arcs4 arcs4(const SweepArgs &a, int v) {
   return r;
 }
 
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS, 1536 / THREADS) k_sweep_rows(SweepArgs a) {
+// MINB CTAs per SM: 1,536 threads per SM by default (40 registers a thread at 512); <512, 4>
+// fits 2,048 threads per SM in 32 registers, for more scattered gathers in flight.
+template <int THREADS, int MINB = 1536 / THREADS>
+__global__ void __launch_bounds__(THREADS, MINB) k_sweep_rows(SweepArgs a) {
   __shared__ SweepShared sh;
   __shared__ int hist[kSortBuckets];
   __shared__ int red[33];
@@ -340,14 +342,21 @@ __global__ void __launch_bounds__(THREADS, 1536 / THREADS) k_sweep_rows(SweepArg
   __syncthreads();
   int L = 0, b = 0, e = 1;
   int32_t *wave = a.lcnt + (size_t)slot * 2 * (a.n_pad + 2);  // the next-list row is free now
+  // The queue is the dependency pass's level queue: wave L (hop layer L) is [wstart[L],
+  // wstart[L + 1]) of it, the starts kept in the far-list row (free now), so that pass needs no
+  // layer sort of its own.
+  int32_t *wstart = wave + (a.n_pad + 2);
   while (b < e) {
-    // a long wave is visited in vertex-id order, staged in the next-list row
+    if (tid == 0) wstart[L] = b;
+    // a long wave is visited in vertex-id order, staged in the next-list row and written back
+    // into the queue in that order (each thread rewrites the entries it visits)
     const bool sorted = e - b >= kSortMinLen;
     if (sorted)
       order_frontier<THREADS>(
           a, [&](int i) { return queue[b + i]; }, e - b, [&](int i) -> int32_t & { return wave[i]; }, hist, red);
     for (int i = b + tid; i < e; i += THREADS) {
       const int v = sorted ? wave[i - b] : queue[i];
+      if (sorted) queue[i] = v;
       const int4 r = rec[v];
       hop[v] = L;
       auto push = [&](int h) {
@@ -375,7 +384,10 @@ __global__ void __launch_bounds__(THREADS, 1536 / THREADS) k_sweep_rows(SweepArg
     if (tid == 0) atomicCAS(a.err, ERR_NONE, ERR_DISCONNECTED);
     return;
   }
-  if (tid == 0 && a.maxhop) a.maxhop[slot] = L - 1;  // waves 0 .. L-1 hold vertices
+  if (tid == 0) {
+    wstart[L] = e;                    // end of the last wave
+    if (a.maxhop) a.maxhop[slot] = L - 1;  // waves 0 .. L-1 hold vertices
+  }
 }
 
 // ------------------------------------------------------------------------------- plain path
@@ -617,6 +629,7 @@ void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop,
   a.sort_buckets = ((d->n_pad - 1) >> a.sort_shift) + 1;
   if (h.tuning.sweep_threads == 256) k_sweep_rows<256><<<ns, 256, 0, st>>>(a);
   else if (h.tuning.sweep_threads == 1024) k_sweep_rows<1024><<<ns, 1024, 0, st>>>(a);
+  else if (h.tuning.sweep_threads == 2048) k_sweep_rows<512, 4><<<ns, 512, 0, st>>>(a);  // 4 x 512 per SM
   else k_sweep_rows<512><<<ns, 512, 0, st>>>(a);
   CK(cudaGetLastError());
 }

@@ -332,7 +332,7 @@ void autotune(Handle &h, const int32_t *sources0, int32_t ns, double *ms_per_sou
       // size, then the Kahn/dependency pass's CTA size
       const int32_t auto_delta = d->sweep_delta_auto;
       for (int32_t mult : {2, 4, 8})  // 0.5x, 1x, 2x the default width (wider and narrower measured slower)
-        for (int32_t threads : {256, 512}) {
+        for (int32_t threads : {256, 512, 2048}) {  // 2048: four 512-thread CTAs per SM
           Tuning t = best;
           t.sweep_delta = std::max(1, auto_delta * mult / 4);
           t.sweep_threads = threads;

@@ -108,6 +108,12 @@ int qbc_index_group_entries(const qbc_index *idx, const int32_t *sources0, int32
  * kernel, 16 for its tall-tree form, 32/K for the general kernel, 0 for the label-free index (the
  * `group` of qbc_index_group_entries).  Needs the index's device state. */
 int qbc_index_label_group(qbc_index *idx, int32_t *sources_per_cta);
+/* Name of the kernel that produces the batched per-source rows under the current tuning
+ * ("k_label_scan_packed", "k_label_scan_rows16", "k_label_scan_tall", "k_label_scan_pair",
+ * "k_label_scan", or "k_sweep_rows" for the label-free index), NUL-terminated in name[0..cap),
+ * for matching profiler output to a configuration; no counterpart in the reference.  Needs the
+ * index's device state. */
+int qbc_index_label_kernel(qbc_index *idx, char *name, int32_t cap);
 void qbc_index_free(qbc_index *idx);
 /* Copies the host index out (for inspection and tests).  Arrays sized by qbc_index_info:
  * vid_of/depth/send[n], lab_off[n+1], dis/anc[info[2]], ch[2*info[2]] (MHL only; may be NULL). */
@@ -130,7 +136,8 @@ int qbc_index_export(const qbc_index *idx, int32_t *vid_of, int32_t *depth, int3
  * rows longer than the tile (0 = 1: one launch, entries beyond the tile read from global memory;
  * 2: one launch per tile of entries, the pairs' running minima kept in the output rows between
  * passes), [10]=distance bucket width of the CSR index's shortest-path sweep (0 = auto: twice the
- * mean arc weight), [11]=threads per CTA of that sweep (256, 512 or 1024; 0 = 512), [12]=sources
+ * mean arc weight), [11]=threads per CTA of that sweep (256, 512 or 1024; 0 = 512; 2048 = 512-thread
+ * CTAs, four per SM), [12]=sources
  * per CTA of the packed-key label scan (32; 16 = the tall-tree kernel: whole rows of 16 sources in
  * shared memory, two targets per warp, target rows streamed through a cp.async ring, when the
  * height fits; 0 = auto: 16 when the 32-source kernel cannot hold whole rows and [7]-[9] are 0),

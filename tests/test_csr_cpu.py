@@ -71,6 +71,8 @@ def test_tuning_fields_round_trip():
     assert t["sweep_delta"] == 500 and t["sweep_threads"] == 512 and t["dep_threads"] == 128
     idx.set_tuning(sweep_threads=1024)
     assert idx.get_tuning()["sweep_threads"] == 1024
+    idx.set_tuning(sweep_threads=2048)  # four 512-thread CTAs per SM
+    assert idx.get_tuning()["sweep_threads"] == 2048
     for bad in (dict(sweep_threads=384), dict(sweep_delta=-1)):
         with pytest.raises(Q.QbcError) as e:
             idx.set_tuning(**bad)

@@ -72,7 +72,7 @@ def test_rows_and_full_bc_shortcut_graphs(n_target, seed, sc):
 
 
 @pytest.mark.parametrize("delta,threads", [(1, 256), (37, 512), (1000, 256), (1 << 20, 512), (0, 512), (0, 1024),
-                                           (1, 1024)])
+                                           (1, 1024), (0, 2048), (37, 2048)])
 def test_bucket_widths_and_threads_give_identical_rows(delta, threads):
     """bucket width 1 (label-setting), the default, and one bucket holding every distance
     (Bellman-Ford on the whole graph) all reach the same fixed point"""
@@ -143,7 +143,7 @@ def test_autotune_keeps_results(g2k):
     srcs = np.arange(0, n, 5, dtype=np.int32)
     before = idx.bc_sources(srcs)
     t = idx.autotune(srcs)
-    assert t["tuning"]["sweep_threads"] in (0, 256, 512)
+    assert t["tuning"]["sweep_threads"] in (0, 256, 512, 2048)
     assert rel_err(idx.bc_sources(srcs), before) <= BC_RTOL
     idx.set_tuning()
 

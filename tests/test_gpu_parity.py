@@ -91,9 +91,11 @@ def test_tall_tree_kernel_forced_2k(g2k, warps, stream):
     idx.set_tuning(label_sources=32)
     try:
         assert idx.label_group() == 32
+        assert idx.label_kernel() == "k_label_scan_packed"
         base = idx.rows(srcs)
         idx.set_tuning(label_sources=16, label_warps=warps, label_stream=stream)
         assert idx.label_group() == 16
+        assert idx.label_kernel() == ("k_label_scan_tall" if stream == 2 else "k_label_scan_rows16")
         alt = idx.rows(srcs)
         bc = idx.bc_sources(srcs)
     finally:
@@ -174,6 +176,27 @@ def test_deep_dag_layer_counters_in_global_memory(form):
         idx.set_tuning()
     i = np.arange(n, dtype=np.float64)
     assert np.allclose(bc, i * (n - 1 - i), rtol=1e-12, atol=0)
+
+
+def test_device_source_list_any_order(g2k):
+    """qbc_bc_sources_device takes the source list in any order, with repeats (it is sorted into
+    tree order on the device): the same BC as the host entry point over the same multiset"""
+    import torch
+
+    n, u, v, w, g, idx, tc, arcs = g2k
+    rng = np.random.default_rng(5)
+    srcs = rng.choice(n, 700, replace=True).astype(np.int32)  # unsorted, with repeats
+    d_src = torch.from_numpy(srcs).to("cuda:0")
+    d_bc = torch.zeros(n, dtype=torch.float64, device="cuda:0")
+    idx.set_tuning(chunk=256)  # several chunks out of the one sorted list
+    try:
+        idx.bc_sources_device(d_src.data_ptr(), int(srcs.shape[0]), d_bc.data_ptr())
+        torch.cuda.synchronize()
+        host = idx.bc_sources(srcs)
+    finally:
+        idx.set_tuning()
+    assert rel_err(d_bc.cpu().numpy(), host) <= BC_RTOL
+    assert rel_err(host, tc.bc(arcs, srcs)) <= BC_RTOL
 
 
 def test_bc_repeatable_and_chunked(g2k):
