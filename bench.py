@@ -272,23 +272,33 @@ def plain_rate(idx, sources, k):
 
 
 # ------------------------------------------------------------------------------- rooflines
+L2_BYTES = 126e6
+
+
 def label_roofline(idx, shard, n, stats, steps, peak, peak_src, sm_mhz):
-    """Dominant kernel of the label path: the packed label scan.  DRAM model per launch: target rows
-    copied once per CTA group of sources (32; 16 for the lane-pair forms), each up to the group's
-    deepest LCA depth (4 B per entry, exact from the index), plus the (dist, count, rho) records
-    and hop layers written (20 B per pair); cross-checked against ncu in
-    profiles/k_label_scan_packed_50k.md (model 9.12 GB, ncu 9.80 GB per 4,096-source launch).  The algorithmic figure of the workload's byte model (12 B
-    per label entry scanned + 12 B per pair) is given as effective_bw: rows are reused by 32
-    sources, so it exceeds the HBM peak."""
+    """Dominant kernel of the label path: the packed label scan.  DRAM model per launch: the target
+    rows' label distances -- read once per launch when the distance array fits in three quarters
+    of the L2 (50k: 69 MB; every CTA group then finds them in L2), else once per CTA group of sources (32;
+    16 for the lane-pair forms), each row up to the group's deepest LCA depth (4 B per entry, exact
+    from the index) -- plus the count/hop gather at each pair's minimising entry (8 B per pair) and
+    the (dist, count, rho) records and hop layers written (20 B per pair).  Cross-checked against
+    ncu in profiles/k_label_scan_packed_50k.md and profiles/k_label_scan_tall_200k.md.  The
+    algorithmic figure of the workload's byte model (12 B per label entry scanned + 12 B per pair)
+    is given as effective_bw: rows are reused by every source of a group, so it exceeds the HBM
+    peak."""
     ns = len(shard)
     per_cta = idx.label_group() or 32
     tall = per_cta == 16
-    group = idx.group_entries(shard, per_cta)
+    dis_bytes = 4.0 * idx.info()[2]
     scan = idx.scan_entries(shard)
     label_ms_step = stats["label_ms"] / steps
     launches_step = max(1.0, stats["label_launches"] / steps)
     launch_ms = label_ms_step / launches_step
-    dram_step = 4.0 * group + 20.0 * ns * n
+    if dis_bytes <= 0.75 * L2_BYTES:
+        rows_step = dis_bytes * launches_step
+    else:
+        rows_step = 4.0 * idx.group_entries(shard, per_cta)
+    dram_step = rows_step + 28.0 * ns * n
     algo_step = 12.0 * scan + 12.0 * ns * n
     achieved = dram_step / launches_step / (launch_ms / 1e3) / 1e9
     effective = algo_step / launches_step / (launch_ms / 1e3) / 1e9

@@ -2264,8 +2264,10 @@ static uint32_t row_wait_spins() {
   return e && *e ? (uint32_t)std::strtoul(e, nullptr, 10) : kRowWaitSpins;
 }
 
+// need_hop false: the caller's next kernel does not read the hop rows (label-free index with the
+// CTA pipelined dependency pass, which walks the sweep's wave queue), so the sweep leaves them out.
 static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t *src, int32_t ns, bool plain,
-                         cudaStream_t st) {
+                         cudaStream_t st, bool need_hop = true) {
   if (h.host.kind == IndexKind::CSR) {  // no labels: shortest-path sweeps give the rows
     std::pair<cudaEvent_t, cudaEvent_t> ev{};
     if (d->profiling) {
@@ -2275,7 +2277,8 @@ static void launch_label(const Handle &h, DeviceState *d, int buf, const int32_t
     if (plain)  // one source over the whole GPU (the buffer's slot 0 has the plain row layout)
       launch_sweep_rows_grid(h, d, d->rec[buf], d->hop[buf], d->order[buf], d->lcnt[buf], src, st);
     else
-      launch_sweep_rows(h, d, d->rec[buf], d->hop[buf], d->order[buf], d->lcnt[buf], d->maxhop[buf], src, ns, st);
+      launch_sweep_rows(h, d, d->rec[buf], d->hop[buf], d->order[buf], d->lcnt[buf], d->maxhop[buf], src, ns, st,
+                        need_hop);
     if (d->profiling) CK(cudaEventRecord(ev.second, st));
     d->label_launches++;
     d->launches++;
@@ -2393,8 +2396,13 @@ static void launch_dep(const Handle &h, DeviceState *d, int buf, const int32_t *
   d->launches++;
 }
 
+// the batched dependency pass of a label-free index reads the wave queue, not the hop rows
+static bool dep_reads_hops(const Handle &h) {
+  return !(h.host.kind == IndexKind::CSR && (h.tuning.dep_form == 0 || h.tuning.dep_form == 4));
+}
+
 void launch_chunk(const Handle &h, DeviceState *d, const int32_t *d_src_tid, int32_t cnt, int buf, cudaStream_t st) {
-  launch_label(h, d, buf, d_src_tid, cnt, false, st);
+  launch_label(h, d, buf, d_src_tid, cnt, false, st, dep_reads_hops(h));
   launch_dep(h, d, buf, d_src_tid, cnt, st);
 }
 
@@ -2683,144 +2691,176 @@ void device_dense_eliminate(int device, DenseTail &dt) {
 struct FillArgs {
   const int32_t *__restrict__ depth;
   const int32_t *__restrict__ parent;
-  const int32_t *__restrict__ send;
   const int64_t *__restrict__ lab_off;
   const int64_t *__restrict__ sep_off;
   const int4 *__restrict__ sep;  // (tid of x, shortcut length, count bits, max hop)
   int32_t *dis;
   int2 *ch;
-  int32_t *anc, *aend;
+  int32_t *anc;  // H2H only: ancestor id of each entry (the H2H fill reads rows of ancestors below x)
 };
 
+// Merge of one separator's candidate into an entry: shorter replaces, equal adds the count and
+// keeps the larger hop (TreeDecomp.cpp:157-193); order-free, so any order of separators gives the
+// sequential merge's entry.
 template <bool MHL>
-__global__ void __launch_bounds__(256) k_fill_level(FillArgs f, const int32_t *__restrict__ nodes, int count) {
-  const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (w >= count) return;
-  const int p = nodes[w];
-  const int h = f.depth[p];
-  const int64_t off = f.lab_off[p];
-  const int par = f.parent[p];
-  const int64_t poff = par >= 0 ? f.lab_off[par] : 0;
-  // ancestor row: the parent's row plus p itself
-  for (int j = lane; j < h; j += 32) {
-    const int a = (j < h - 1) ? f.anc[poff + j] : p;
-    f.anc[off + j] = a;
-    f.aend[off + j] = f.send[a];
-  }
-  __syncwarp();
-  const int64_t sb = f.sep_off[p], se = f.sep_off[p + 1];
-  for (int j = lane; j < h - 1; j += 32) {
-    int best = kInfDist;
-    unsigned c = 0;
-    int hp = 0;
-    const int64_t ajoff = MHL ? 0 : f.lab_off[f.anc[off + j]];
-    for (int64_t i = sb; i < se; i++) {
-      const int4 x = f.sep[i];
-      const int k = f.depth[x.x] - 1;
-      int nd;
-      unsigned nc = 0;
-      int nh = 0;
-      if (j <= k) {  // ancestor j is x or above x: x's own row
-        const int64_t xo = f.lab_off[x.x] + j;
-        nd = x.y + f.dis[xo];
-        if (MHL) {
-          const int2 cx = f.ch[xo];
-          nc = (unsigned)x.z * (unsigned)cx.x;
-          nh = x.w + cx.y;
-        }
-      } else if (!MHL) {  // H2H true distances: ancestor j lies below x, its row holds x
-        nd = x.y + f.dis[ajoff + k];
-      } else {
-        continue;
-      }
-      if (nd < best) {
-        best = nd;
-        c = nc;
-        hp = nh;
-      } else if (MHL && nd == best) {
-        c += nc;
-        hp = max(hp, nh);
-      }
-    }
-    f.dis[off + j] = best;
-    if (MHL) f.ch[off + j] = make_int2((int)c, hp);
-  }
-  if (lane == 0) {
-    f.dis[off + h - 1] = 0;
-    if (MHL) f.ch[off + h - 1] = make_int2(1, 0);
+__device__ __forceinline__ void fill_merge(int &best, unsigned &c, int &hp, int nd, unsigned nc, int nh) {
+  if (nd < best) {
+    best = nd;
+    c = nc;
+    hp = nh;
+  } else if (MHL && nd == best) {
+    c += nc;
+    hp = max(hp, nh);
   }
 }
 
-// The same fill for nodes with large separators (near the root): one CTA per node, the separator
-// entries with their vertices' row offsets and depths staged in shared memory, threads over the
-// row's entries.  A warp per node there spends its time on dependent per-separator loads.
-constexpr int kBigSeparator = 32;  // separators of at least this size take the CTA form
-constexpr int kFillStageBytes = 28;  // shared bytes per staged separator entry
+// Entries of a row filled per thread: the separator entries' row loads are issued kFillBatch at a
+// time before any is merged, so a thread waits for one round of L2/DRAM latency per batch instead
+// of one per separator vertex (the loop was latency-bound: 1M build, 2.9 s of fill kernels).
+constexpr int kFillBatch = 8;
+constexpr int kFillWarpSpan = 128;  // row entries per warp task of k_fill_level
 
+// A separator entry as the fill reads it: (shortcut length, count bits, max hop), the vertex's
+// row offset and depth - 1.
+struct FillSep {
+  int len;
+  unsigned cnt;
+  int hop, k;
+  long long xoff;
+};
+
+// Entry j of a row from separator entries sep(0..nx): MHL reads x's own row at j (ancestors of x
+// at depth > k contribute nothing); H2H reads, for ancestors j below x, the ancestor's row at k.
+template <bool MHL, class GET>
+__device__ __forceinline__ void fill_entry(const FillArgs &f, int j, int64_t ajoff, int nx, GET sep, int &best,
+                                           unsigned &c, int &hp) {
+  for (int i0 = 0; i0 < nx; i0 += kFillBatch) {
+    int dv[kFillBatch];
+    int2 cv[kFillBatch];
+    FillSep x[kFillBatch];
+#pragma unroll
+    for (int q = 0; q < kFillBatch; q++) {
+      x[q] = sep(min(i0 + q, nx - 1));
+      const bool in = i0 + q < nx;
+      const bool own = j <= x[q].k;
+      const bool use = in && (own || !MHL);
+      const int64_t xo = own ? x[q].xoff + j : ajoff + x[q].k;
+      dv[q] = use ? f.dis[xo] : 0;
+      if (MHL) cv[q] = use ? f.ch[xo] : make_int2(0, 0);
+      if (!use) x[q].k = INT_MIN;  // marks the slot unused
+    }
+#pragma unroll
+    for (int q = 0; q < kFillBatch; q++) {
+      if (x[q].k == INT_MIN) continue;
+      if (MHL)
+        fill_merge<true>(best, c, hp, x[q].len + dv[q], x[q].cnt * (unsigned)cv[q].x, x[q].hop + cv[q].y);
+      else
+        fill_merge<false>(best, c, hp, x[q].len + dv[q], 0u, 0);
+    }
+  }
+}
+
+// One launch per tree depth k (all its nodes have rows of k entries); a warp takes one node's
+// entries [span * kFillWarpSpan, ...) so that long rows of few nodes still spread over many warps.
+// The node's separator entries (fewer than kBigSeparator here, else as many as needed) are staged
+// 32 at a time in registers, lane i holding entry i, and handed round by shuffles.
 template <bool MHL>
-__global__ void __launch_bounds__(256) k_fill_node_cta(FillArgs f, const int32_t *__restrict__ nodes) {
-  extern __shared__ int4 fsm[];
-  const int p = nodes[blockIdx.x];
+__global__ void __launch_bounds__(256) k_fill_level(FillArgs f, const int32_t *__restrict__ nodes, int count, int spans) {
+  const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (w >= count * spans) return;
+  const int p = nodes[w / spans];
+  const int jlo = (w % spans) * kFillWarpSpan;
   const int h = f.depth[p];
+  if (jlo >= h) return;
+  const int jhi = min(h, jlo + kFillWarpSpan);
   const int64_t off = f.lab_off[p];
-  const int par = f.parent[p];
-  const int64_t poff = par >= 0 ? f.lab_off[par] : 0;
+  if (!MHL) {  // H2H: ancestor ids of this span (the parent's row plus p), read below by the same lane
+    const int par = f.parent[p];
+    const int64_t poff = par >= 0 ? f.lab_off[par] : 0;
+    for (int j = jlo + lane; j < jhi; j += 32) f.anc[off + j] = (j < h - 1) ? f.anc[poff + j] : p;
+  }
   const int64_t sb = f.sep_off[p];
   const int nx = (int)(f.sep_off[p + 1] - sb);
-  int4 *s_sep = fsm;
-  int64_t *s_xoff = reinterpret_cast<int64_t *>(s_sep + nx);
-  int32_t *s_k = reinterpret_cast<int32_t *>(s_xoff + nx);
-  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-    const int4 x = f.sep[sb + i];
-    s_sep[i] = x;
-    s_xoff[i] = f.lab_off[x.x];
-    s_k[i] = f.depth[x.x] - 1;
-  }
-  for (int j = threadIdx.x; j < h; j += blockDim.x) {  // ancestor row: the parent's plus p itself
-    const int a = (j < h - 1) ? f.anc[poff + j] : p;
-    f.anc[off + j] = a;
-    f.aend[off + j] = f.send[a];
-  }
-  __syncthreads();
-  for (int j = threadIdx.x; j < h - 1; j += blockDim.x) {
+  for (int jb = jlo; jb < jhi; jb += 32) {
+    const int j = jb + lane;
+    const bool live = j < h - 1;
     int best = kInfDist;
     unsigned c = 0;
     int hp = 0;
-    const int64_t ajoff = MHL ? 0 : f.lab_off[f.anc[off + j]];
-    for (int i = 0; i < nx; i++) {
-      const int4 x = s_sep[i];
-      const int k = s_k[i];
-      int nd;
-      unsigned nc = 0;
-      int nh = 0;
-      if (j <= k) {
-        const int64_t xo = s_xoff[i] + j;
-        nd = x.y + f.dis[xo];
-        if (MHL) {
-          const int2 cx = f.ch[xo];
-          nc = (unsigned)x.z * (unsigned)cx.x;
-          nh = x.w + cx.y;
-        }
-      } else if (!MHL) {
-        nd = x.y + f.dis[ajoff + k];
-      } else {
-        continue;
+    const int64_t ajoff = (!MHL && live) ? f.lab_off[f.anc[off + j]] : 0;
+    for (int base = 0; base < nx; base += 32) {
+      FillSep mine{0, 0u, 0, -1, 0};
+      if (base + lane < nx) {
+        const int4 xs = f.sep[sb + base + lane];
+        mine = FillSep{xs.y, (unsigned)xs.z, xs.w, f.depth[xs.x] - 1, (long long)f.lab_off[xs.x]};
       }
-      if (nd < best) {
-        best = nd;
-        c = nc;
-        hp = nh;
-      } else if (MHL && nd == best) {
-        c += nc;
-        hp = max(hp, nh);
+      const int cnt = min(32, nx - base);
+      auto get = [&](int i) {
+        return FillSep{__shfl_sync(kFull, mine.len, i), (unsigned)__shfl_sync(kFull, (int)mine.cnt, i),
+                       __shfl_sync(kFull, mine.hop, i), __shfl_sync(kFull, mine.k, i),
+                       __shfl_sync(kFull, mine.xoff, i)};
+      };
+      // every lane runs the batches (the shuffles need the whole warp); lanes past the row's last
+      // separator-filled entry merge nothing
+      int b2 = best;
+      unsigned c2 = c;
+      int h2 = hp;
+      fill_entry<MHL>(f, live ? j : 0, ajoff, cnt, get, b2, c2, h2);
+      if (live) {
+        best = b2;
+        c = c2;
+        hp = h2;
       }
     }
+    if (live) {
+      f.dis[off + j] = best;
+      if (MHL) f.ch[off + j] = make_int2((int)c, hp);
+    } else if (j == h - 1) {  // p's own entry
+      f.dis[off + j] = 0;
+      if (MHL) f.ch[off + j] = make_int2(1, 0);
+    }
+  }
+}
+
+// The same fill for nodes with large separators (near the root): a CTA per (node, block of
+// blockDim.x entries), the separator entries with their vertices' row offsets and depths staged
+// in shared memory, a thread per entry.
+constexpr int kBigSeparator = 32;  // separators of at least this size take the CTA form
+constexpr int kFillStageBytes = 24;  // shared bytes per staged separator entry (FillSep)
+
+template <bool MHL>
+__global__ void __launch_bounds__(256) k_fill_node_cta(FillArgs f, const int32_t *__restrict__ nodes) {
+  extern __shared__ FillSep fsm_sep[];
+  const int p = nodes[blockIdx.y];
+  const int h = f.depth[p];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if ((int)(blockIdx.x * blockDim.x) >= h) return;  // whole CTA, before the barrier
+  const int64_t off = f.lab_off[p];
+  const int64_t sb = f.sep_off[p];
+  const int nx = (int)(f.sep_off[p + 1] - sb);
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    const int4 x = f.sep[sb + i];
+    fsm_sep[i] = FillSep{x.y, (unsigned)x.z, x.w, f.depth[x.x] - 1, (long long)f.lab_off[x.x]};
+  }
+  int64_t ajoff = 0;
+  if (!MHL && j < h) {  // H2H: this entry's ancestor (the parent's row plus p), read below by this thread
+    const int par = f.parent[p];
+    const int64_t poff = par >= 0 ? f.lab_off[par] : 0;
+    const int a = (j < h - 1) ? f.anc[poff + j] : p;
+    f.anc[off + j] = a;
+    ajoff = f.lab_off[a];
+  }
+  __syncthreads();
+  if (j < h - 1) {
+    int best = kInfDist;
+    unsigned c = 0;
+    int hp = 0;
+    fill_entry<MHL>(f, j, ajoff, nx, [&](int i) { return fsm_sep[i]; }, best, c, hp);
     f.dis[off + j] = best;
     if (MHL) f.ch[off + j] = make_int2((int)c, hp);
-  }
-  if (threadIdx.x == 0) {
-    f.dis[off + h - 1] = 0;
-    if (MHL) f.ch[off + h - 1] = make_int2(1, 0);
+  } else if (j == h - 1) {
+    f.dis[off + j] = 0;
+    if (MHL) f.ch[off + j] = make_int2(1, 0);
   }
 }
 
@@ -2980,7 +3020,7 @@ void device_build(Handle &h, int device, const Separators &seps) {
       d = new_state(h, device);
       CK(cudaStreamSynchronize(d->s_label));
     }
-    auto t_fill = std::make_unique<TraceScope>("row buffers and device row fill");
+    auto t_fill = std::make_unique<TraceScope>("row buffers and separator upload");
     cudaStream_t st = d->s_label;
     const int64_t L = ix.lab_off[ix.n];
     d->dis = dmalloc<int32_t>(d, (size_t)L);
@@ -2992,8 +3032,9 @@ void device_build(Handle &h, int device, const Separators &seps) {
       CK(cudaMemsetAsync(d->ch, 0, (size_t)L * 8, st));
     }
     // nodes grouped by depth (counting sort; preorder keeps each level in increasing tid order);
-    // within a level, nodes with small separators first (warp per node), then large ones (CTA per
-    // node, separators staged in shared memory; beyond the staging capacity they stay warp-filled)
+    // within a level, nodes with small separators first (a warp per 128 entries of a node's row),
+    // then large ones (a CTA per 256 entries, separators staged in shared memory; beyond the
+    // staging capacity they stay warp-filled)
     const int64_t stage_cap = std::max(kBigSeparator, (d->smem_optin - 1024) / kFillStageBytes);
     auto big = [&](int32_t t) {
       const int64_t nx = seps.off[t + 1] - seps.off[t];
@@ -3018,23 +3059,23 @@ void device_build(Handle &h, int device, const Separators &seps) {
         else nodes[fs[ix.depth[t]]++] = t;
       }
     }
-    // temporaries of the fill, freed at the end
-    // per-entry ancestor ids and subtree ends (f_anc, f_aend): needed while rows are filled (a row
-    // reads its ancestors' entries), freed with the other temporaries once the fill is done
-    int32_t *d_nodes = nullptr, *d_max = nullptr, *f_anc = nullptr, *f_aend = nullptr;
+    // temporaries of the fill, freed at the end; per-entry ancestor ids (f_anc) only for H2H,
+    // whose fill reads rows of ancestors below a separator vertex (MHL rows read only the
+    // separator vertices' own rows)
+    int32_t *d_nodes = nullptr, *d_max = nullptr, *f_anc = nullptr;
     int64_t *d_soff = nullptr;
     int4 *d_sep = nullptr;
     auto free_tmp = [&] {
-      void *q[] = {d_nodes, d_max, d_soff, d_sep, f_anc, f_aend};
+      void *q[] = {d_nodes, d_max, d_soff, d_sep, f_anc};
       for (void *p : q)
         if (p) cudaFree(p);
     };
     try {
       CK(cudaMalloc(&d_nodes, nodes.size() * 4));
-      CK(cudaMalloc(&f_anc, (size_t)std::max<int64_t>(L, 1) * 4));
-      CK(cudaMalloc(&f_aend, (size_t)std::max<int64_t>(L, 1) * 4));
-      CK(cudaMemsetAsync(f_anc, 0, (size_t)L * 4, st));
-      CK(cudaMemsetAsync(f_aend, 0, (size_t)L * 4, st));
+      if (!mhl) {
+        CK(cudaMalloc(&f_anc, (size_t)std::max<int64_t>(L, 1) * 4));
+        CK(cudaMemsetAsync(f_anc, 0, (size_t)L * 4, st));
+      }
       CK(cudaMalloc(&d_soff, seps.off.size() * 8));
       CK(cudaMalloc(&d_sep, std::max<size_t>(16, seps.ent.size() * 4)));
       CK(cudaMalloc(&d_max, 4));
@@ -3042,22 +3083,28 @@ void device_build(Handle &h, int device, const Separators &seps) {
       CK(cudaMemcpyAsync(d_soff, seps.off.data(), seps.off.size() * 8, cudaMemcpyHostToDevice, st));
       if (!seps.ent.empty()) CK(cudaMemcpyAsync(d_sep, seps.ent.data(), seps.ent.size() * 4, cudaMemcpyHostToDevice, st));
       CK(cudaMemsetAsync(d_max, 0, 4, st));
-      FillArgs f{d->depth, d->parent, d->send, d->lab_off, d_soff, d_sep, d->dis, d->ch, f_anc, f_aend};
+      FillArgs f{d->depth, d->parent, d->lab_off, d_soff, d_sep, d->dis, d->ch, f_anc};
+      if (TraceScope::enabled()) {  // split the phase: buffers and upload, then the fill kernels
+        CK(cudaStreamSynchronize(st));
+        t_fill = std::make_unique<TraceScope>("device row fill kernels");
+      }
       const size_t max_stage = (size_t)stage_cap * kFillStageBytes;
       CK(cudaFuncSetAttribute(k_fill_node_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_stage));
       CK(cudaFuncSetAttribute(k_fill_node_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_stage));
       for (int32_t k = 1; k <= ix.tree_height; k++) {
         const int count = (int)(lvl[k + 1] - lvl[k] - nbig[k]);
         if (count > 0) {
-          const int blocks = (count + 7) / 8;
-          if (mhl) k_fill_level<true><<<blocks, 256, 0, st>>>(f, d_nodes + lvl[k], count);
-          else k_fill_level<false><<<blocks, 256, 0, st>>>(f, d_nodes + lvl[k], count);
+          const int spans = (k + kFillWarpSpan - 1) / kFillWarpSpan;  // rows at depth k have k entries
+          const int blocks = (int)(((int64_t)count * spans + 7) / 8);
+          if (mhl) k_fill_level<true><<<blocks, 256, 0, st>>>(f, d_nodes + lvl[k], count, spans);
+          else k_fill_level<false><<<blocks, 256, 0, st>>>(f, d_nodes + lvl[k], count, spans);
           CK(cudaGetLastError());
         }
         if (nbig[k] > 0) {
           const size_t smem = (size_t)maxsep[k] * kFillStageBytes;
-          if (mhl) k_fill_node_cta<true><<<(unsigned)nbig[k], 256, smem, st>>>(f, d_nodes + lvl[k + 1] - nbig[k]);
-          else k_fill_node_cta<false><<<(unsigned)nbig[k], 256, smem, st>>>(f, d_nodes + lvl[k + 1] - nbig[k]);
+          const dim3 grid((unsigned)((k + 255) / 256), (unsigned)nbig[k]);
+          if (mhl) k_fill_node_cta<true><<<grid, 256, smem, st>>>(f, d_nodes + lvl[k + 1] - nbig[k]);
+          else k_fill_node_cta<false><<<grid, 256, smem, st>>>(f, d_nodes + lvl[k + 1] - nbig[k]);
           CK(cudaGetLastError());
         }
       }
@@ -3205,7 +3252,7 @@ void device_bc_sources(Handle &h, const int32_t *d_sources0, int32_t ns, double 
   for (int32_t off = 0; off < ns; off += d->chunk) {
     const int b = 0;  // stream order frees the buffer for the next chunk
     const int32_t cnt = std::min(d->chunk, ns - off);
-    launch_label(h, d, b, tids + off, cnt, false, d->s_label);
+    launch_label(h, d, b, tids + off, cnt, false, d->s_label, dep_reads_hops(h));
     // The dependency pass runs right after the scan on the same stream: run concurrently on a
     // second stream the two kernels thrash each other's caches and both slow down ~2x.
     launch_dep(h, d, b, tids + off, cnt, d->s_label);

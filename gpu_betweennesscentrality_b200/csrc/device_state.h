@@ -143,8 +143,10 @@ void launch_chunk(const Handle &h, DeviceState *d, const int32_t *d_src_tid, int
 // CSR index: rows of ns sources by shortest-path sweeps into the given scratch (rec/hop/order/lcnt
 // laid out as a buffer of ns slots), one CTA per source (sssp.cu): records (dist, count, 0), hop
 // layers and, when maxhop is not null, the largest layer per source -- the label scan's outputs.
+// write_hop false: hop layers are left out (the hop row is still the sweep's staging space); the
+// CTA pipelined dependency pass does not read them, it walks the wave queue.
 void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop, int32_t *order, int32_t *lcnt,
-                       int32_t *maxhop, const int32_t *src, int32_t ns, cudaStream_t st);
+                       int32_t *maxhop, const int32_t *src, int32_t ns, cudaStream_t st, bool write_hop = true);
 int32_t sweep_delta(const Handle &h, const DeviceState *d);
 // CSR index, plain path: one source's rows (slot 0 of a one-slot buffer; no largest-layer output)
 // by a cooperative launch of the whole GPU

@@ -61,6 +61,7 @@ struct SweepArgs {
   int32_t *err;
   int32_t sort_shift;    // frontier lists are visited in order of v >> sort_shift ...
   int32_t sort_buckets;  // ... (n_pad - 1) >> sort_shift < sort_buckets <= kSortBuckets
+  int32_t write_hop;     // 0: hop layers not written (the dependency pass reads the wave queue)
 };
 
 constexpr int kSortBuckets = 4096;  // shared-memory counters of the frontier ordering
@@ -358,7 +359,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_sweep_rows(SweepArgs a) {
       const int v = sorted ? wave[i - b] : queue[i];
       if (sorted) queue[i] = v;
       const int4 r = rec[v];
-      hop[v] = L;
+      if (a.write_hop) hop[v] = L;  // a scattered 4-byte write: skipped when no one reads it
       auto push = [&](int h) {
         int4 &rh = rec[h];
         atomicAdd(&rh.y, r.y);                                            // 32-bit wrapping, as count_t
@@ -607,7 +608,7 @@ int32_t sweep_delta(const Handle &h, const DeviceState *d) {
 }
 
 void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop, int32_t *order, int32_t *lcnt,
-                       int32_t *maxhop, const int32_t *src, int32_t ns, cudaStream_t st) {
+                       int32_t *maxhop, const int32_t *src, int32_t ns, cudaStream_t st, bool write_hop) {
   SweepArgs a{};
   a.arc4 = d->arc4;
   a.arc_hw = d->arc_hw;
@@ -624,6 +625,7 @@ void launch_sweep_rows(const Handle &h, DeviceState *d, int4 *rec, int32_t *hop,
   a.lcnt = lcnt;
   a.maxhop = maxhop;
   a.err = d->err;
+  a.write_hop = write_hop ? 1 : 0;
   a.sort_shift = 0;
   while (((d->n_pad - 1) >> a.sort_shift) >= kSortBuckets) a.sort_shift++;
   a.sort_buckets = ((d->n_pad - 1) >> a.sort_shift) + 1;
