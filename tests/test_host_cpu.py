@@ -192,7 +192,7 @@ def test_min_degree_order_is_permutation():
 def test_min_degree_order_rule(n, seed, shortcuts):
     """the elimination takes the vertex of least current degree (fill-in included), the smaller id
     on ties -- restated here with neighbour sets and checked step by step (the library keeps the
-    remaining vertices in an indexed heap and merges large separators on several threads)"""
+    remaining vertices in one id bitmap per degree and merges large separators on several threads)"""
     n, u, v, w = grid_lines(n, seed=seed, shortcut_frac=shortcuts)
     g = Q.Graph()
     g.ReadLines(n, u, v, w)
