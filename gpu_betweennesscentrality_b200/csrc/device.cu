@@ -2603,6 +2603,192 @@ __global__ void __launch_bounds__(256) k_dense_update(int4 *M, int32_t *deg, int
   }
 }
 
+// The whole tail in one cooperative launch (1,024-thread CTAs, all resident): the same
+// pick, compaction and update per step, separated by grid barriers instead of kernel boundaries
+// (two launches per step cost ~38 us a step at 1M).  The grid is small -- 32 CTAs when they cover
+// the row's columns, so a barrier has few arrivals; a step's update takes a warp per separator
+// vertex, about 1,000 at most on the 1M grid -- and the barrier polls without sleeping.  Every CTA
+// finds the pick from the per-CTA minima; the compaction of row x is split by column ranges, each
+// CTA placing its entries after those of the CTAs before it; data written by other CTAs is read
+// through L2 (__ldcg).  A barrier wait is bounded (a few million polls, ~1-2 s); when it runs out
+// the grid leaves at its next barrier and the host reports the error.
+struct DenseCtl {
+  unsigned arrive, gen;
+  int abort, err;
+};
+constexpr long long kDenseSpinLimit = 1ll << 22;  // polls of the generation word per barrier wait (~1-2 s)
+
+__device__ __forceinline__ bool dense_grid_sync(DenseCtl *c, unsigned &gen) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    if (atomicAdd(&c->arrive, 1u) == gridDim.x - 1) {
+      c->arrive = 0;
+      __threadfence();
+      atomicExch(&c->gen, gen + 1);
+    } else {
+      long long spins = 0;
+      while (*(volatile unsigned *)&c->gen == gen) {
+        if (*(volatile int *)&c->abort || ++spins > kDenseSpinLimit) {
+          ok = 0;
+          break;
+        }
+      }
+      if (!ok) {
+        atomicExch(&c->abort, 1);
+        atomicExch(&c->err, 1);
+      }
+    }
+    gen++;
+    __threadfence();
+    s_ok = ok && !*(volatile int *)&c->abort;
+  }
+  __syncthreads();
+  return s_ok;
+}
+
+constexpr int kTailThreads = 1024;
+
+__device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v, unsigned long long *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v = min(v, __shfl_xor_sync(kFull, v, o));
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  v = red[lane];  // kTailThreads / 32 == 32 partials
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v = min(v, __shfl_xor_sync(kFull, v, o));
+  __syncthreads();
+  return v;
+}
+
+// exclusive prefix sum of x over the CTA's kTailThreads threads; *total = the CTA's sum
+__device__ __forceinline__ int block_scan_excl(int x, int *red, int *total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) red[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int w = red[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, w, o);
+      if (lane >= o) w += y;
+    }
+    red[lane] = w;  // inclusive warp totals
+  }
+  __syncthreads();
+  const int r = incl - x + (warp > 0 ? red[warp - 1] : 0);
+  *total = red[31];
+  __syncthreads();
+  return r;
+}
+
+// r <= gridDim.x * kTailThreads (one column of row x per thread in the compaction)
+__global__ void __launch_bounds__(kTailThreads, 1) k_dense_tail(int4 *M, int32_t *deg, uint8_t *alive, int32_t r,
+                                                                int32_t *order, int4 *xlist, int4 *sep,
+                                                                int64_t *sep_off, unsigned long long *part_best,
+                                                                int32_t *part_cnt, DenseCtl *ctl) {
+  __shared__ unsigned long long s_red64[32];
+  __shared__ int s_red[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int G = gridDim.x, b = blockIdx.x;
+  const int cols = (r + G - 1) / G;
+  const int c_lo = min(r, b * cols), c_hi = min(r, c_lo + cols);
+  unsigned gen = 0;
+  int64_t so = 0;  // separator entries written by the steps before (the same in every CTA)
+  for (int s = 0; s < r; s++) {
+    // pick: the live vertex of least (degree, id)
+    unsigned long long best = ~0ull;
+    for (int i = b * kTailThreads + tid; i < r; i += G * kTailThreads)
+      if (__ldcg(alive + i)) best = min(best, ((unsigned long long)(uint32_t)__ldcg(deg + i) << 32) | (uint32_t)i);
+    best = block_min_u64(best, s_red64);
+    if (tid == 0) part_best[b] = best;
+    if (!dense_grid_sync(ctl, gen)) return;
+    best = ~0ull;
+    for (int i = tid; i < G; i += kTailThreads) best = min(best, __ldcg(part_best + i));
+    best = block_min_u64(best, s_red64);
+    const int x = (int)(best & 0xffffffffu);
+    // row x compacted in column order: this CTA's columns [c_lo, c_hi), one per thread
+    const int c = c_lo + tid;
+    int4 e = make_int4(kAbsentLen, 0, 0, 0);
+    if (c < c_hi) e = __ldcg(M + (int64_t)x * r + c);
+    const int pres = e.x != kAbsentLen;
+    int mine_total = 0;
+    const int my_off = block_scan_excl(pres, s_red, &mine_total);
+    if (tid == 0) part_cnt[b] = mine_total;
+    if (!dense_grid_sync(ctl, gen)) return;
+    int before = 0, all = 0;
+    for (int i = tid; i < G; i += kTailThreads) {
+      const int v = __ldcg(part_cnt + i);
+      all += v;
+      if (i < b) before += v;
+    }
+    before = __reduce_add_sync(kFull, before);
+    all = __reduce_add_sync(kFull, all);
+    if (lane == 0) {
+      s_red[warp] = before;
+      s_red64[warp] = (unsigned long long)all;
+    }
+    __syncthreads();
+    before = 0;
+    all = 0;
+    for (int w = 0; w < kTailThreads / 32; w++) {
+      before += s_red[w];
+      all += (int)s_red64[w];
+    }
+    __syncthreads();
+    if (pres) {
+      const int4 v = make_int4(c, e.x, e.y, e.z);
+      xlist[before + my_off] = v;
+      sep[so + before + my_off] = v;
+    }
+    if (b == 0 && tid == 0) {
+      order[s] = x;
+      alive[x] = 0;
+      sep_off[s + 1] = so + all;
+    }
+    so += all;
+    if (!dense_grid_sync(ctl, gen)) return;
+    // update: a warp per separator vertex u, the shortcuts through x to every other one
+    const int k = all;
+    for (int i = b * (kTailThreads / 32) + warp; i < k; i += G * (kTailThreads / 32)) {
+      const int4 a = __ldcg(xlist + i);
+      int4 *row = M + (int64_t)a.x * r;
+      int added = 0;
+      for (int j = lane; j < k; j += 32) {
+        if (j == i) continue;
+        const int4 bb = __ldcg(xlist + j);
+        const int nl = a.y + bb.y;
+        const int nc = (int)((unsigned)a.z * (unsigned)bb.z);
+        const int nh = a.w + bb.w;
+        const int4 cur = __ldcg(row + bb.x);
+        if (cur.x == kAbsentLen) {
+          row[bb.x] = make_int4(nl, nc, nh, 0);
+          added++;
+        } else if (nl < cur.x) {
+          row[bb.x] = make_int4(nl, nc, nh, 0);
+        } else if (nl == cur.x) {
+          row[bb.x] = make_int4(cur.x, (int)((unsigned)cur.y + (unsigned)nc), max(cur.z, nh), 0);
+        }
+      }
+      added = __reduce_add_sync(kFull, added);
+      if (lane == 0) {
+        row[x] = make_int4(kAbsentLen, 0, 0, 0);
+        deg[a.x] = __ldcg(deg + a.x) + added - 1;
+      }
+    }
+    if (!dense_grid_sync(ctl, gen)) return;
+  }
+}
+
 // device buffers freed on every exit of the function that owns them
 struct DevBufs {
   std::vector<void *> p;
@@ -2666,9 +2852,31 @@ void device_dense_eliminate(int device, DenseTail &dt) {
   k_dense_clear<<<148 * 8, 256, 0, st>>>(M, (int64_t)r * r);
   k_dense_scatter<<<148 * 8, 256, 0, st>>>(M, r, row, ent, m);
   CK(cudaGetLastError());
-  for (int32_t s = 0; s < r; s++) {
-    k_dense_pick<<<1, kPickThreads, 0, st>>>(M, deg, alive, r, s, order, xlist, xcount, sep, sep_off);
-    k_dense_update<<<148 * 4, 256, 0, st>>>(M, deg, r, xlist, xcount, order, s);
+  // one cooperative launch for all r steps when one CTA per SM fits and covers the row's columns;
+  // else two launches per step
+  int per_sm = 0, sms = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dense_tail, kTailThreads, 0));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  int coop = 0;
+  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+  const int grid = std::min(sms, std::max(32, (int)((r + kTailThreads - 1) / kTailThreads)));
+  if (coop && per_sm >= 1 && (int64_t)grid * kTailThreads >= r) {
+    unsigned long long *part_best = buf.get<unsigned long long>((size_t)grid);
+    int32_t *part_cnt = buf.get<int32_t>((size_t)grid);
+    DenseCtl *ctl = buf.get<DenseCtl>(1);
+    CK(cudaMemsetAsync(ctl, 0, sizeof(DenseCtl), st));
+    int32_t rr = r;
+    void *args[] = {&M, &deg, &alive, &rr, &order, &xlist, &sep, &sep_off, &part_best, &part_cnt, &ctl};
+    CK(cudaLaunchCooperativeKernel((const void *)k_dense_tail, dim3((unsigned)grid), dim3(kTailThreads), args, 0, st));
+    DenseCtl hc{};
+    CK(cudaMemcpyAsync(&hc, ctl, sizeof(DenseCtl), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (hc.err || hc.abort) throw Error(QBC_ECUDA, "dense elimination: a grid barrier wait ran out");
+  } else {
+    for (int32_t s = 0; s < r; s++) {
+      k_dense_pick<<<1, kPickThreads, 0, st>>>(M, deg, alive, r, s, order, xlist, xcount, sep, sep_off);
+      k_dense_update<<<148 * 4, 256, 0, st>>>(M, deg, r, xlist, xcount, order, s);
+    }
   }
   CK(cudaGetLastError());
   dt.order.resize((size_t)r);
@@ -3201,8 +3409,6 @@ void check_err(DeviceState *d) {
 }
 
 // ------------------------------------------------------------------------------- drivers
-// Sorts nothing on the device: chunks take the source list in the given order; sources listed in
-// increasing tid order group nearby tree nodes into one CTA.
 // A device source list as tids in tree order, on stream st: the label kernels give consecutive
 // sources to one CTA, and sources of one subtree share most of their ancestors, so a CTA's scans
 // end at similar depths and its target rows are fetched to similar depths (1M grid, 4,096 random
