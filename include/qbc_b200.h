@@ -174,7 +174,10 @@ int qbc_bc_sources(qbc_index *idx, const int32_t *sources0, int32_t ns, double *
 int qbc_bc_plain(qbc_index *idx, const int32_t *sources0, int32_t ns, double *bc_out);
 /* Device-resident variant: d_sources0 (ns int32) and d_bc (n doubles, accumulated into, not
  * cleared) are device pointers; stream is a cudaStream_t or NULL for the index's own stream.
- * Returns after enqueueing; the caller synchronises. */
+ * Sources may come in any order and repeat: they are sorted into tree order on the device (the
+ * label kernels run fastest on tree neighbours); the index grows its source buffers (2 x 4 B per
+ * source plus the sort's temporary storage) when a longer list arrives, which synchronises the
+ * stream once.  Returns after enqueueing; the caller synchronises. */
 int qbc_bc_sources_device(qbc_index *idx, const int32_t *d_sources0, int32_t ns, double *d_bc, void *stream);
 
 /* One source's BC contribution without allocating: no counterpart in the reference.
