@@ -327,21 +327,22 @@ def label_roofline(idx, shard, n, stats, steps, peak, peak_src, sm_mhz):
 
 def sweep_roofline(n, ns_step, stats, steps, peak, peak_src):
     """The label-free sweep kernel (k_sweep_rows).  DRAM model per source: each 16-byte record is
-    initialised (16 B), read and rewritten by the in-degree pass (32 B), and the hop layer written
-    (4 B) -- 52 B per vertex; the frontier phases' scattered record visits come on top (one DRAM
-    sector per visit at this size), which ncu's traffic in profiles/ shows."""
+    initialised (16 B), then read and rewritten by the in-degree pass (32 B) -- 48 B per vertex (the
+    batched sweep writes no hop layers: the dependency pass reads its wave queue); the frontier
+    phases' scattered record visits come on top (DRAM sectors per visit), which ncu's traffic in
+    profiles/ shows (~415 B per (source, vertex) at 200k + 2 %)."""
     ms_step = stats["label_ms"] / steps
     launches_step = max(1.0, stats["label_launches"] / steps)
     launch_ms = ms_step / launches_step
-    dram_step = 52.0 * n * ns_step
+    dram_step = 48.0 * n * ns_step
     achieved = dram_step / launches_step / (launch_ms / 1e3) / 1e9
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "peak_source": peak_src, "kernel": "k_sweep_rows",
             "dram_model_bytes_per_launch": dram_step / launches_step, "launch_ms": launch_ms,
             "launches_per_step": launches_step, "sweep_ms_per_step": ms_step,
             "dependency_ms_per_step": stats["dep_ms"] / steps,
-            "note": "model = 52 B per (source, vertex): record init, in-degree pass read + write, hop layer; the "
-                    "scattered frontier visits are latency-bound gathers (DRAM sectors, not bytes)"}
+            "note": "model = 48 B per (source, vertex): record init, in-degree pass read + write; the scattered "
+                    "frontier visits are gathers of DRAM sectors (ncu: ~415 B per (source, vertex) moved)"}
 
 
 # ------------------------------------------------------------------------------- RQ (batched / served)
