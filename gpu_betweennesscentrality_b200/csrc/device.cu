@@ -2476,13 +2476,15 @@ void device_set_chunk(Handle &h, int32_t chunk) {
 // The last r vertices of the min-degree elimination (TreeDecomp.cpp:54-208 semantics, as the host's
 // eliminate): near the root the separators are large (hundreds of vertices) and the host spends
 // most of its time there on the k^2 shortcut updates of each step.  Here the remaining graph is a
-// dense r x r matrix of (length, count bits, max hop) entries, absent = kAbsentLen, and each step
-// is two launches: k_dense_pick (one CTA: the live vertex of minimum (degree, id), its row
-// compacted into the separator list in column order) and k_dense_update (one warp per separator
-// vertex u: the shortcuts through x to every other separator vertex, with the host's rule -- a
-// shorter length replaces, an equal one adds the count and keeps the larger hop -- then u's entry
-// for x removed).  The picks, separators and so the tree and rows are the host elimination's: the
-// separator order differs (column order here) and nothing downstream depends on it.
+// dense r x r matrix of (length, count bits, max hop) entries, absent = kAbsentLen.  A step picks
+// the live vertex x of minimum (degree, id), compacts its row into the separator list in column
+// order, and updates every separator vertex u (a warp each): the shortcuts through x to every
+// other separator vertex, with the host's rule -- a shorter length replaces, an equal one adds the
+// count and keeps the larger hop -- then u's entry for x removed.  All steps run in one
+// cooperative launch (k_dense_tail below); where that cannot be resident, each step is two
+// launches, k_dense_pick and k_dense_update.  The picks, separators and so the tree and rows are
+// the host elimination's: the separator order differs (column order here) and nothing downstream
+// depends on it.
 constexpr int32_t kAbsentLen = 0x7fffffff;
 
 __global__ void k_dense_clear(int4 *M, int64_t count) {
